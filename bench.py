@@ -1,0 +1,466 @@
+"""Benchmark of the B200 diffuse path tracer through its C ABI.
+
+Headline workload (one step): the ~1.38M-triangle terrain scene (1024x512-quad
+heightfield + 256 level-3 icospheres), 1920x1080, 64 spp, maxDepth 5, rendered
+by one prt_render call.  Metric: Mrays/s, rays counted as the reference counts
+them (one per closest-hit query).  Synthetic, seeded scene data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank renders its own replica of the workload with
+its own pass range (weak scaling, no collective on the data path); the timed
+region is bracketed by barriers and the max over ranks is reported.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "embree-benchmark-protoray_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "Mrays/s 1080p 64spp"
+UNIT = "Mrays/s"
+W, H, SPP, DEPTH = 1920, 1080, 64, 5
+ALGO_BYTES_PER_RAY = 192   # compulsory wavefront record traffic per ray
+L2_BYTES = 126 * 1024 * 1024
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per ray of the bounce kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_bounce_terrain1080p.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_ray="):
+            try:
+                return float(line.split("=", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[2:6]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world, local, backend):
+    import torch
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local) if backend == "nccl" else None)
+    return dist if world > 1 else None
+
+
+def max_over_ranks(x, dist, device):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, dist, device):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None):
+    """Times the reference's own diffuseStream renderer (oracle/_ref) on the
+    host cores at 1920x1080, maxDepth 5; one step = `frames_per_step` frames."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import scenes
+    if not oracle.Reference.available():
+        return None
+    mesh, view = scenes.terrain_scene()
+    import tempfile
+    d = tempfile.mkdtemp(prefix="prt_bench_")
+    path = scenes.write_scene(d, "terrain", mesh, view)
+    R = oracle.Reference()
+    rs = R.open(path)
+    rs.build(1)
+    cores = int(os.environ.get("PRT_REF_THREADS", "0")) or (os.cpu_count() or 1)
+    for _ in range(warmup):
+        rs.render("diffuseStream", view, W, H, frames_per_step, DEPTH, accel=1, want_sums=False)
+    rays = 0.0
+    secs = 0.0
+    t0 = time.perf_counter()
+    n = 0
+    while n < steps:
+        _, st = rs.render("diffuseStream", view, W, H, frames_per_step, DEPTH, accel=1, want_sums=False)
+        rays += st["rays"]
+        secs += st["seconds"]
+        n += 1
+        if sample_seconds and time.perf_counter() - t0 > sample_seconds:
+            break
+    wall = time.perf_counter() - t0
+    return {"value": rays / 1e6 / secs, "rays": rays, "seconds": secs, "wall": wall, "frames": n * frames_per_step,
+            "cores": cores, "cpu": cpu_model()}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    r = cpu_reference_run(args.steps, args.warmup)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libprotoray_ref.so was not built"}))
+        return 0
+    sample = (f"reference diffuseStream renderer (stream 2048, AVX2, GCC -O3) with the project FP32 SAH BVH "
+              f"standing in for Embree 3 (absent); terrain scene 1920x1080, {r['frames']} frames x 1 spp, "
+              f"maxDepth {DEPTH}; {r['cpu']}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(r["value"], 3), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * r["seconds"] / max(1, r["frames"]), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "terrain 1.38M tris, 1920x1080, maxDepth 5 (1 spp per step)", "width": W,
+                   "height": H, "maxDepth": DEPTH},
+        "cpu_baseline": {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(r["value"], 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def make_ctx(prt, mesh, device):
+    c = prt.Context(device)
+    c.load_mesh(mesh.indices, mesh.positions)
+    b = c.build()
+    return c, b
+
+
+def batch_workload(scenes, seed=7, n=64):
+    """64 requests: W,H in U{128..1024} rounded to multiples of 8, spp U{1..64},
+    maxDepth 5, over 8 seeded scenes of 10K-2M triangles."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        w = int(rng.integers(128, 1025)) // 8 * 8
+        h = int(rng.integers(128, 1025)) // 8 * 8
+        reqs.append({"scene": int(rng.integers(0, 8)), "width": w, "height": h, "spp": int(rng.integers(1, 65)),
+                     "maxDepth": 5})
+    return reqs
+
+
+def run_batch(prt, torch, device, reps=2):
+    import scenes
+    ctxs, views = [], []
+    for k in range(8):
+        m, v = scenes.batch_scene(k)
+        c, _ = make_ctx(prt, m, device)
+        ctxs.append(c)
+        views.append(v)
+    work = batch_workload(scenes)
+    reqs = []
+    for q in work:
+        acc = torch.zeros((q["height"], q["width"], 4), dtype=torch.float32, device=f"cuda:{device}")
+        reqs.append({"scene": ctxs[q["scene"]], "camera": prt.camera_from_view(views[q["scene"]], q["width"], q["height"]),
+                     "width": q["width"], "height": q["height"], "spp": q["spp"], "maxDepth": q["maxDepth"],
+                     "accum": acc})
+    batcher = ctxs[0]
+    batcher.render_batch(reqs)   # warm-up (graph capture)
+    best_b = None
+    for _ in range(reps):
+        st = batcher.render_batch(reqs)
+        best_b = st if best_b is None or st["ms"] < best_b["ms"] else best_b
+    # the same requests as sequential plain launches
+    seq_ms, seq_rays = 0.0, 0
+    for q in work:
+        c = ctxs[q["scene"]]
+        c.init_frame(q["width"], q["height"])
+        c.set_view(views[q["scene"]], q["width"], q["height"])
+    for rep in range(reps + 1):
+        ms, rays = 0.0, 0
+        for q in work:
+            c = ctxs[q["scene"]]
+            c.init_frame(q["width"], q["height"])
+            c.set_view(views[q["scene"]], q["width"], q["height"])
+            st = c.render(q["spp"], q["maxDepth"], accumulate=False)
+            ms += st["ms"]
+            rays += st["ray"]
+        if rep > 0 and (seq_ms == 0 or ms < seq_ms):
+            seq_ms, seq_rays = ms, rays
+    out = {"batched_mray": round(best_b["mray"], 2), "sequential_mray": round(seq_rays / 1e6 / (seq_ms / 1e3), 2),
+           "batched_ms": round(best_b["ms"], 2), "sequential_ms": round(seq_ms, 2), "requests": len(work),
+           "rays": int(best_b["ray"])}
+    out["speedup"] = round(out["batched_mray"] / out["sequential_mray"], 3)
+    for c in ctxs:
+        c.close()
+    return out
+
+
+def run_fwd_bwd(prt, torch, device):
+    """512x512, 16 spp, small scene with per-triangle albedo U[0.2,0.8]:
+    forward render and path-replay backward of an L2 image loss."""
+    import scenes
+    mesh, view = scenes.small_scene()
+    c, _ = make_ctx(prt, mesh, device)
+    alb = torch.from_numpy(scenes.albedo_for(mesh)).to(f"cuda:{device}")
+    c.set_albedo(alb)
+    Wd, Hd, spp, depth = 512, 512, 16, 5
+    c.init_frame(Wd, Hd)
+    c.set_view(view, Wd, Hd)
+    g = torch.randn((Hd, Wd, 3), dtype=torch.float32, device=f"cuda:{device}")
+    d_alb = torch.zeros(mesh.tri_count, dtype=torch.float32, device=f"cuda:{device}")
+    d_sky = torch.zeros(1, dtype=torch.float32, device=f"cuda:{device}")
+    for _ in range(2):
+        c.clear()
+        c.render(spp, depth, accumulate=False)
+        c.render_backward(0, spp, depth, g, d_alb, d_sky)
+    torch.cuda.synchronize()
+    fw, fb = [], []
+    for _ in range(3):
+        c.clear()
+        t0 = time.perf_counter()
+        st = c.render(spp, depth, accumulate=False)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        c.render_backward(0, spp, depth, g, d_alb, d_sky)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        fw.append(st["ms"])
+        fb.append(st["ms"] + (t2 - t1) * 1e3)
+    c.close()
+    f, b = min(fw), min(fb)
+    return {"fwd_ms": round(f, 3), "fwd_bwd_ms": round(b, 3), "ratio": round(b / f, 3),
+            "config": "small scene 82K tris, 512x512, 16 spp, maxDepth 5, per-triangle albedo"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and fwd+bwd measurements")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local = dist_env()
+    import torch
+    import prt
+    import scenes
+    torch.cuda.set_device(local)
+    dist = init_dist(world, local, "nccl")
+    dev = f"cuda:{local}"
+
+    mesh, view = scenes.terrain_scene()
+    ctx, build = make_ctx(prt, mesh, local)
+    ctx.init_frame(W, H)
+    ctx.set_view(view, W, H)
+
+    # L2 flush buffer (written between timed steps)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def step(pass_base):
+        ctx.set_pass(pass_base)
+        return ctx.render(SPP, DEPTH, accumulate=False)
+
+    for w in range(args.warmup):
+        step(rank * SPP)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    launches0 = ctx.launch_count()
+    rays, ms = 0, 0.0
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            flush.fill_(float(s))
+            torch.cuda.synchronize()
+            st = step(rank * SPP)
+            rays += st["ray"]
+            ms += st["ms"]
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        wall = time.perf_counter() - t0
+    launches = ctx.launch_count() - launches0
+    ms_max = max_over_ranks(ms, dist, dev)
+    rays_all = sum_over_ranks(rays, dist, dev)
+    value = rays_all / 1e6 / (ms_max / 1e3)
+
+    # end-to-end through the C ABI with host buffers: camera in, image out
+    host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    cam = prt.camera_from_view(view, W, H)
+    ctx.set_camera(cam)
+    step(rank * SPP)
+    ctx.read_accum(host_img)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e_rays = 0
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        ctx.set_camera(cam)
+        st = step(rank * SPP)
+        ctx.read_accum(host_img)
+        e_rays += st["ray"]
+    torch.cuda.synchronize()
+    e_secs = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e_value = sum_over_ranks(e_rays, dist, dev) / 1e6 / e_secs
+
+    hbm, peak_kind = peaks()
+    achieved = value * 1e6 * ALGO_BYTES_PER_RAY / 1e9 / max(1, world)   # per GPU
+    tr = profile_traffic()
+    rays_per_step = rays / args.steps
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
+                "traffic": None if tr is None else round(tr * rays_per_step),
+                "algorithmic_bytes_per_ray": ALGO_BYTES_PER_RAY,
+                "per": "render step (the k_bounce launches of one 64-spp frame, >99% of its device time)"}
+    if tr is not None:
+        roofline["traffic_bytes_per_ray"] = tr
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras["batched"] = run_batch(prt, torch, local)
+        extras["differentiable"] = run_fwd_bwd(prt, torch, local)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference_run(1000, 1, sample_seconds=args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic seeded scene (no public dataset)",
+            "config": {"workload": "terrain: 1024x512-quad heightfield + 256 level-3 icospheres, 1,376,256 tris; "
+                                   "1920x1080, 64 spp, maxDepth 5", "width": W, "height": H, "spp": SPP,
+                       "maxDepth": DEPTH, "triangles": mesh.tri_count, "l2": "flushed between timed steps",
+                       "parallelism": f"replicas{world}", "buildMs": round(build["buildMs"], 2),
+                       "buildMprim": round(build["buildMprim"], 2), "bvh8_nodes": build["nodeCount"],
+                       "bvh8_levels": build["levels"]},
+            "rays_per_step": int(rays / args.steps),
+            "wall_s": round(wall, 3),
+            "e2e": {"value": round(e_value, 2), "unit": UNIT, "h2d_bytes_per_step": 76,
+                    "d2h_bytes_per_step": W * H * 16},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "clocks": clocks.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {
+                "value": round(cpu["value"], 3), "unit": UNIT, "cores": cpu["cores"], "kind": "reference",
+                "sample": (f"reference diffuseStream renderer + project FP32 SAH BVH (Embree 3 absent), terrain "
+                           f"scene 1920x1080, {cpu['frames']} frames x 1 spp, maxDepth 5, {cpu['wall']:.1f} s; "
+                           f"{cpu['cpu']}")}
+        line.update(extras)
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

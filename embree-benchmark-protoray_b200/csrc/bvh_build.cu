@@ -1,0 +1,743 @@
+// GPU LBVH build into the compressed 8-wide node layout of prt_device.cuh.
+//
+// Replaces the acceleration-structure build of the reference's GPU path
+// (OptiX Prime model->setTriangles/update, accel/optix/optix_intersector_stream_cuda.cpp:49-59;
+// Embree rtcCommitScene on the CPU, accel/embree/embree_intersector.cpp:65-85).
+//
+// Steps (all on the device):
+//   1. triangle boxes + centroid bounds (block partials, one final reduce)
+//   2. 30-bit Morton codes of the centroids (10 bits per axis)
+//   3. stable LSD radix sort of (code, triangle) pairs, 4-bit digits
+//   4. binary radix tree over the sorted codes (Karras, HPG 2012); equal
+//      codes are ordered by their position, so duplicates are handled
+//   5. bottom-up bounds refit (second child to arrive computes the union)
+//   6. top-down collapse into 8-wide nodes, one tree level per launch:
+//      children are opened greedily by largest surface area while fewer than
+//      8 exist; subtrees of <= 3 triangles become leaves; child slots are
+//      assigned so that slot s holds the child nearest the origin of rays in
+//      direction octant s; child boxes are quantized to 8 bits per axis.
+#include <algorithm>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "prt_device.cuh"
+#include "prt_internal.h"
+
+namespace prt_b200 {
+
+namespace {
+
+constexpr int kSortBlock = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortBlock * kSortItems;
+constexpr int kRadixBits = 4;
+constexpr int kRadix = 1 << kRadixBits;
+
+struct Box6
+{
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ uint32_t expand10(uint32_t v)
+{
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// --- 1. triangle boxes and centroid bounds --------------------------------
+
+__global__ void k_tri_boxes(const float* __restrict__ pos, const int* __restrict__ idx, int nt, float* __restrict__ triBox,
+                            float* __restrict__ partial)
+{
+    float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nt; p += gridDim.x * blockDim.x)
+    {
+        int i0 = idx[3 * p], i1 = idx[3 * p + 1], i2 = idx[3 * p + 2];
+        float lo[3], hi[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            float a = pos[3 * i0 + k], b = pos[3 * i1 + k], c = pos[3 * i2 + k];
+            lo[k] = fminf(a, fminf(b, c));
+            hi[k] = fmaxf(a, fmaxf(b, c));
+            triBox[6 * (size_t)p + k] = lo[k];
+            triBox[6 * (size_t)p + 3 + k] = hi[k];
+            float cc = 0.5f * (lo[k] + hi[k]);
+            clo[k] = fminf(clo[k], cc);
+            chi[k] = fmaxf(chi[k], cc);
+        }
+    }
+    __shared__ float s[6][256];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        s[k][threadIdx.x] = clo[k];
+        s[3 + k][threadIdx.x] = chi[k];
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1)
+    {
+        if ((int)threadIdx.x < w)
+        {
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                s[k][threadIdx.x] = fminf(s[k][threadIdx.x], s[k][threadIdx.x + w]);
+                s[3 + k][threadIdx.x] = fmaxf(s[3 + k][threadIdx.x], s[3 + k][threadIdx.x + w]);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_reduce_bounds(const float* __restrict__ partial, int nblocks, float* __restrict__ out)
+{
+    __shared__ float s[6][256];
+    float v[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        for (int k = 0; k < 3; ++k)
+        {
+            v[k] = fminf(v[k], partial[6 * b + k]);
+            v[3 + k] = fmaxf(v[3 + k], partial[6 * b + 3 + k]);
+        }
+    for (int k = 0; k < 6; ++k) s[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1)
+    {
+        if ((int)threadIdx.x < w)
+            for (int k = 0; k < 3; ++k)
+            {
+                s[k][threadIdx.x] = fminf(s[k][threadIdx.x], s[k][threadIdx.x + w]);
+                s[3 + k][threadIdx.x] = fmaxf(s[3 + k][threadIdx.x], s[3 + k][threadIdx.x + w]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
+// --- 2. Morton codes -------------------------------------------------------
+
+__global__ void k_morton(const float* __restrict__ triBox, int nt, const float* __restrict__ cb, uint32_t* __restrict__ keys,
+                         uint32_t* __restrict__ vals)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nt) return;
+    uint32_t code = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        float c = 0.5f * (triBox[6 * (size_t)p + k] + triBox[6 * (size_t)p + 3 + k]);
+        float ext = cb[3 + k] - cb[k];
+        float u = ext > 0.f ? (c - cb[k]) / ext : 0.f;
+        uint32_t q = (uint32_t)fminf(fmaxf(u * 1024.0f, 0.0f), 1023.0f);
+        code |= expand10(q) << k;
+    }
+    keys[p] = code;
+    vals[p] = (uint32_t)p;
+}
+
+// --- 3. radix sort (stable LSD, 4-bit digits) -----------------------------
+
+__global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift,
+                                                        uint32_t* __restrict__ hist, int nblocks)
+{
+    __shared__ uint32_t h[kRadix];
+    if (threadIdx.x < kRadix) h[threadIdx.x] = 0;
+    __syncthreads();
+    int base = blockIdx.x * kSortTile;
+    for (int k = 0; k < kSortItems; ++k)
+    {
+        int i = base + k * kSortBlock + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < kRadix) hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// exclusive scan of hist (kRadix * nblocks entries, digit-major) in one block
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* __restrict__ hist, int count)
+{
+    __shared__ uint32_t part[1024];
+    int per = (count + 1023) / 1024;
+    int b0 = threadIdx.x * per, b1 = min(count, b0 + per);
+    uint32_t sum = 0;
+    for (int i = b0; i < b1; ++i) sum += hist[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1)
+    {
+        uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+    for (int i = b0; i < b1; ++i)
+    {
+        uint32_t v = hist[i];
+        hist[i] = run;
+        run += v;
+    }
+}
+
+// Each thread owns kSortItems consecutive keys of the tile; per-thread digit
+// counts are scanned block-wide in (digit, thread) order, which gives every
+// key its stable rank within the tile.
+__global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint32_t* __restrict__ keysIn,
+                                                           const uint32_t* __restrict__ valsIn, uint32_t* __restrict__ keysOut,
+                                                           uint32_t* __restrict__ valsOut, int n, int shift,
+                                                           const uint32_t* __restrict__ hist, int nblocks)
+{
+    __shared__ uint32_t cnt[kRadix * kSortBlock];   // [digit][thread]
+    __shared__ uint32_t warpSum[kSortBlock / 32];
+    __shared__ uint32_t digitStart[kRadix];
+    const int t = threadIdx.x;
+    const int base = blockIdx.x * kSortTile + t * kSortItems;
+    uint32_t key[kSortItems], val[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k)
+    {
+        int i = base + k;
+        key[k] = i < n ? keysIn[i] : 0xffffffffu;
+        val[k] = i < n ? valsIn[i] : 0u;
+    }
+#pragma unroll
+    for (int d = 0; d < kRadix; ++d) cnt[d * kSortBlock + t] = 0;
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k)
+        if (base + k < n) cnt[((key[k] >> shift) & (kRadix - 1)) * kSortBlock + t]++;
+    __syncthreads();
+    // block-wide exclusive scan over cnt[] (kRadix * kSortBlock entries):
+    // thread t scans entries [t*kRadix, (t+1)*kRadix) sequentially
+    uint32_t local[kRadix];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < kRadix; ++j)
+    {
+        local[j] = cnt[t * kRadix + j];
+        sum += local[j];
+    }
+    // scan of per-thread sums
+    uint32_t x = sum;
+    const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
+    {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warpSum[warp] = x;
+    __syncthreads();
+    if (warp == 0)
+    {
+        uint32_t w = lane < kSortBlock / 32 ? warpSum[lane] : 0u;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        if (lane < kSortBlock / 32) warpSum[lane] = w;
+    }
+    __syncthreads();
+    uint32_t excl = x - sum + (warp ? warpSum[warp - 1] : 0u);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kRadix; ++j)
+    {
+        cnt[t * kRadix + j] = excl;
+        excl += local[j];
+    }
+    __syncthreads();
+    if (t < kRadix) digitStart[t] = cnt[t * kSortBlock];
+    __syncthreads();
+    uint32_t seen[kRadix];
+#pragma unroll
+    for (int d = 0; d < kRadix; ++d) seen[d] = 0;
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k)
+    {
+        if (base + k >= n) continue;
+        uint32_t d = (key[k] >> shift) & (kRadix - 1);
+        uint32_t rankInTile = cnt[d * kSortBlock + t] + seen[d];
+#pragma unroll
+        for (int dd = 0; dd < kRadix; ++dd)
+            if (dd == (int)d) seen[dd]++;
+        uint32_t dst = hist[d * nblocks + blockIdx.x] + (rankInTile - digitStart[d]);
+        keysOut[dst] = key[k];
+        valsOut[dst] = val[k];
+    }
+}
+
+// --- 4. Karras binary radix tree --------------------------------------------
+
+__device__ __forceinline__ int delta(const uint32_t* __restrict__ keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    uint32_t a = keys[i], b = keys[j];
+    if (a != b) return __clz(a ^ b);
+    return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+}
+
+// internal nodes 0..n-2; child encoding: >= 0 internal, < 0 leaf ~k
+__global__ void k_karras(const uint32_t* __restrict__ keys, int n, int2* __restrict__ child, int2* __restrict__ range,
+                         int* __restrict__ parent)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s = 0;
+    int t = l;
+    do
+    {
+        t = (t + 1) >> 1;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    int gamma = i + s * d + min(d, 0);
+    int lo = min(i, j), hi = max(i, j);
+    int left = (lo == gamma) ? ~gamma : gamma;
+    int right = (hi == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    child[i] = make_int2(left, right);
+    range[i] = make_int2(lo, hi);
+    // parents: internal nodes at [0, n-1), leaves at [n-1, 2n-1)
+    parent[left >= 0 ? left : (n - 1) + ~left] = i;
+    parent[right >= 0 ? right : (n - 1) + ~right] = i;
+    if (i == 0) parent[0] = -1;
+}
+
+// --- 5. bottom-up refit -----------------------------------------------------
+
+__global__ void k_refit(int n, const uint32_t* __restrict__ vals, const float* __restrict__ triBox,
+                        const int2* __restrict__ child, const int* __restrict__ parent, float* box, int* flag)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    // leaf box
+    uint32_t p = vals[k];
+    float* lb = box + 6 * (size_t)((n - 1) + k);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) lb[c] = triBox[6 * (size_t)p + c];
+    int node = parent[(n - 1) + k];
+    while (node >= 0)
+    {
+        __threadfence();
+        if (atomicAdd(&flag[node], 1) == 0) return;   // the sibling finishes this node
+        int2 ch = child[node];
+        int a = ch.x >= 0 ? ch.x : (n - 1) + ~ch.x;
+        int b = ch.y >= 0 ? ch.y : (n - 1) + ~ch.y;
+        float r[6];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+        {
+            r[c] = fminf(__ldcg(box + 6 * (size_t)a + c), __ldcg(box + 6 * (size_t)b + c));
+            r[3 + c] = fmaxf(__ldcg(box + 6 * (size_t)a + 3 + c), __ldcg(box + 6 * (size_t)b + 3 + c));
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) __stcg(box + 6 * (size_t)node + c, r[c]);
+        node = parent[node];
+    }
+}
+
+// --- 6. collapse into 8-wide nodes ------------------------------------------
+
+struct CollapseArgs
+{
+    int n;
+    const int2* child;
+    const int2* range;
+    const float* box;
+    const uint32_t* vals;
+    const float* pos;
+    const int* idx;
+    Bvh8Node* nodes;
+    TriRec* tris;
+    int* nodeCounter;
+    int* triCounter;
+    int nodeCapacity;
+    int* error;
+};
+
+__device__ __forceinline__ int ref_count(const CollapseArgs& a, int ref)
+{
+    if (ref < 0) return 1;
+    int2 r = a.range[ref];
+    return r.y - r.x + 1;
+}
+
+__device__ __forceinline__ const float* ref_box(const CollapseArgs& a, int ref)
+{
+    return a.box + 6 * (size_t)(ref >= 0 ? ref : (a.n - 1) + ~ref);
+}
+
+__device__ __forceinline__ float half_area(const float* b)
+{
+    float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Work item: (binary reference, 8-wide node index).  A binary reference of
+// ~0 with n == 1 is the single-triangle scene.
+__global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int workCount, int2* __restrict__ next,
+                           int* __restrict__ nextCount)
+{
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= workCount) return;
+    int bref = work[w].x;
+    int nodeIdx = work[w].y;
+
+    int ch[8];
+    int nc;
+    if (bref < 0)
+    {
+        ch[0] = bref;
+        nc = 1;
+    }
+    else
+    {
+        int2 c = a.child[bref];
+        ch[0] = c.x;
+        ch[1] = c.y;
+        nc = 2;
+        while (nc < 8)
+        {
+            int best = -1;
+            float bestA = -1.f;
+            for (int i = 0; i < nc; ++i)
+            {
+                if (ch[i] < 0 || ref_count(a, ch[i]) <= 3) continue;
+                float ar = half_area(ref_box(a, ch[i]));
+                if (ar > bestA) { bestA = ar; best = i; }
+            }
+            if (best < 0) break;
+            int2 c2 = a.child[ch[best]];
+            ch[best] = c2.x;
+            ch[nc++] = c2.y;
+        }
+    }
+
+    // node box = union of child boxes
+    float nb[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float cen[8][3];
+    for (int i = 0; i < nc; ++i)
+    {
+        const float* b = ref_box(a, ch[i]);
+        for (int k = 0; k < 3; ++k)
+        {
+            nb[k] = fminf(nb[k], b[k]);
+            nb[3 + k] = fmaxf(nb[3 + k], b[3 + k]);
+            cen[i][k] = 0.5f * (b[k] + b[3 + k]);
+        }
+    }
+
+    // slot assignment: greedy on cost(slot s, child c) = projection of the
+    // child centroid on the direction of octant s (smaller = nearer)
+    int slotOf[8];
+    int childInSlot[8];
+    for (int s = 0; s < 8; ++s) childInSlot[s] = -1;
+    for (int i = 0; i < nc; ++i) slotOf[i] = -1;
+    for (int it = 0; it < nc; ++it)
+    {
+        float bestC = FLT_MAX;
+        int bs = -1, bc = -1;
+        for (int s = 0; s < 8; ++s)
+        {
+            if (childInSlot[s] >= 0) continue;
+            float dx = (s & 1) ? -1.f : 1.f, dy = (s & 2) ? -1.f : 1.f, dz = (s & 4) ? -1.f : 1.f;
+            for (int i = 0; i < nc; ++i)
+            {
+                if (slotOf[i] >= 0) continue;
+                float c = cen[i][0] * dx + cen[i][1] * dy + cen[i][2] * dz;
+                if (c < bestC) { bestC = c; bs = s; bc = i; }
+            }
+        }
+        childInSlot[bs] = bc;
+        slotOf[bc] = bs;
+    }
+
+    // allocate internal children (in slot order) and leaf triangles
+    int nInternal = 0, nTris = 0;
+    for (int i = 0; i < nc; ++i)
+    {
+        int cnt = ref_count(a, ch[i]);
+        if (cnt > 3) nInternal++;
+        else nTris += cnt;
+    }
+    int childBase = nInternal ? atomicAdd(a.nodeCounter, nInternal) : 0;
+    int triBase = nTris ? atomicAdd(a.triCounter, nTris) : 0;
+    if (childBase + nInternal > a.nodeCapacity)
+    {
+        atomicExch(a.error, 1);
+        return;
+    }
+
+    // header: origin + per-axis power-of-two scale with 255 steps
+    uint32_t ebits[3];
+    float scale[3];
+    for (int k = 0; k < 3; ++k)
+    {
+        float ext = nb[3 + k] - nb[k];
+        int e = -100;
+        if (ext > 0.f)
+        {
+            e = (int)ceilf(log2f(ext / 255.0f));
+            while (ldexpf(255.0f, e) < ext) ++e;
+        }
+        e = max(e, -126);
+        e = min(e, 127);
+        ebits[k] = (uint32_t)(e + 127);
+        scale[k] = ldexpf(1.0f, e);
+    }
+    uint8_t meta[8], qlo[3][8], qhi[3][8];
+    uint32_t imask = 0;
+    int internalRank = 0, triOff = 0;
+    for (int s = 0; s < 8; ++s)
+    {
+        int i = childInSlot[s];
+        if (i < 0)
+        {
+            meta[s] = 0;
+            for (int k = 0; k < 3; ++k) { qlo[k][s] = 255; qhi[k][s] = 0; }
+            continue;
+        }
+        const float* b = ref_box(a, ch[i]);
+        for (int k = 0; k < 3; ++k)
+        {
+            double lo = floor(((double)b[k] - (double)nb[k]) / (double)scale[k]);
+            double hi = ceil(((double)b[3 + k] - (double)nb[k]) / (double)scale[k]);
+            qlo[k][s] = (uint8_t)fmax(0.0, fmin(255.0, lo));
+            qhi[k][s] = (uint8_t)fmax(0.0, fmin(255.0, hi));
+        }
+        int cnt = ref_count(a, ch[i]);
+        if (cnt > 3)
+        {
+            meta[s] = (uint8_t)(0x20 | (24 + s));
+            imask |= 1u << s;
+            int2 item = make_int2(ch[i], childBase + internalRank);
+            internalRank++;
+            int slotQ = atomicAdd(nextCount, 1);
+            next[slotQ] = item;
+        }
+        else
+        {
+            uint32_t unary = (1u << cnt) - 1u;
+            meta[s] = (uint8_t)((unary << 5) | (uint32_t)triOff);
+            // copy the triangles of the leaf (a contiguous sorted range)
+            int first = ch[i] < 0 ? ~ch[i] : a.range[ch[i]].x;
+            for (int k = 0; k < cnt; ++k)
+            {
+                uint32_t prim = a.vals[first + k];
+                int i0 = a.idx[3 * prim], i1 = a.idx[3 * prim + 1], i2 = a.idx[3 * prim + 2];
+                TriRec tr;
+                tr.v0 = make_float4(a.pos[3 * i0], a.pos[3 * i0 + 1], a.pos[3 * i0 + 2], __int_as_float((int)prim));
+                tr.v1 = make_float4(a.pos[3 * i1], a.pos[3 * i1 + 1], a.pos[3 * i1 + 2], 0.f);
+                tr.v2 = make_float4(a.pos[3 * i2], a.pos[3 * i2 + 1], a.pos[3 * i2 + 2], 0.f);
+                a.tris[triBase + triOff + k] = tr;
+            }
+            triOff += cnt;
+        }
+    }
+    auto pack4 = [](const uint8_t* v) {
+        return (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
+    };
+    Bvh8Node node;
+    node.q[0] = make_uint4(__float_as_uint(nb[0]), __float_as_uint(nb[1]), __float_as_uint(nb[2]),
+                           ebits[0] | (ebits[1] << 8) | (ebits[2] << 16) | (imask << 24));
+    node.q[1] = make_uint4((uint32_t)childBase, (uint32_t)triBase, pack4(meta), pack4(meta + 4));
+    node.q[2] = make_uint4(pack4(qlo[0]), pack4(qlo[0] + 4), pack4(qlo[1]), pack4(qlo[1] + 4));
+    node.q[3] = make_uint4(pack4(qlo[2]), pack4(qlo[2] + 4), pack4(qhi[0]), pack4(qhi[0] + 4));
+    node.q[4] = make_uint4(pack4(qhi[1]), pack4(qhi[1] + 4), pack4(qhi[2]), pack4(qhi[2] + 4));
+    a.nodes[nodeIdx] = node;
+}
+
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+} // namespace
+
+#define BUILD_CHECK(x)                                                                                          \
+    do                                                                                                         \
+    {                                                                                                          \
+        cudaError_t e_ = (x);                                                                                  \
+        if (e_ != cudaSuccess)                                                                                 \
+        {                                                                                                      \
+            err = std::string(#x) + ": " + cudaGetErrorString(e_);                                              \
+            status = PRT_ECUDA;                                                                                \
+            goto done;                                                                                         \
+        }                                                                                                      \
+    } while (0)
+
+int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
+               std::string& err, BuildInfo* info)
+{
+    (void)nv;
+    int status = PRT_OK;
+    out.release();
+    if (nt <= 0) return PRT_OK;   // empty scene: no root
+
+    const int n = nt;
+    const int nInternal = n > 1 ? n - 1 : 0;
+    const int sortBlocks = div_up(n, kSortTile);
+    const int histCount = kRadix * sortBlocks;
+    const int boundBlocks = std::min(1024, div_up(n, 256));
+    const int nodeCapacity = std::max(1, nInternal);
+
+    float* triBox = nullptr;
+    float* partial = nullptr;
+    float* cbounds = nullptr;
+    uint32_t *keysA = nullptr, *keysB = nullptr, *valsA = nullptr, *valsB = nullptr, *hist = nullptr;
+    int2 *child = nullptr, *range = nullptr, *workA = nullptr, *workB = nullptr;
+    int *parent = nullptr, *flag = nullptr, *counters = nullptr;
+    float* box = nullptr;
+    int hostCounters[4];
+    int levels = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    BUILD_CHECK(cudaEventCreate(&ev0));
+    BUILD_CHECK(cudaEventCreate(&ev1));
+    BUILD_CHECK(cudaEventRecord(ev0, stream));
+
+    BUILD_CHECK(cudaMalloc(&triBox, sizeof(float) * 6 * (size_t)n));
+    BUILD_CHECK(cudaMalloc(&partial, sizeof(float) * 6 * (size_t)boundBlocks));
+    BUILD_CHECK(cudaMalloc(&cbounds, sizeof(float) * 6));
+    BUILD_CHECK(cudaMalloc(&keysA, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(cudaMalloc(&keysB, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(cudaMalloc(&valsA, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(cudaMalloc(&valsB, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(cudaMalloc(&hist, sizeof(uint32_t) * (size_t)histCount));
+    BUILD_CHECK(cudaMalloc(&child, sizeof(int2) * (size_t)std::max(1, nInternal)));
+    BUILD_CHECK(cudaMalloc(&range, sizeof(int2) * (size_t)std::max(1, nInternal)));
+    BUILD_CHECK(cudaMalloc(&parent, sizeof(int) * (size_t)(2 * n)));
+    BUILD_CHECK(cudaMalloc(&flag, sizeof(int) * (size_t)std::max(1, nInternal)));
+    BUILD_CHECK(cudaMalloc(&box, sizeof(float) * 6 * (size_t)(2 * n)));
+    BUILD_CHECK(cudaMalloc(&workA, sizeof(int2) * (size_t)nodeCapacity));
+    BUILD_CHECK(cudaMalloc(&workB, sizeof(int2) * (size_t)nodeCapacity));
+    BUILD_CHECK(cudaMalloc(&counters, sizeof(int) * 4));
+    BUILD_CHECK(cudaMalloc(&out.nodes, sizeof(Bvh8Node) * (size_t)nodeCapacity));
+    BUILD_CHECK(cudaMalloc(&out.tris, sizeof(TriRec) * (size_t)n));
+
+    k_tri_boxes<<<boundBlocks, 256, 0, stream>>>(dPos, dIdx, n, triBox, partial);
+    k_reduce_bounds<<<1, 256, 0, stream>>>(partial, boundBlocks, cbounds);
+    k_morton<<<div_up(n, 256), 256, 0, stream>>>(triBox, n, cbounds, keysA, valsA);
+    for (int shift = 0; shift < 32; shift += kRadixBits)
+    {
+        k_sort_hist<<<sortBlocks, kSortBlock, 0, stream>>>(keysA, n, shift, hist, sortBlocks);
+        k_sort_scan<<<1, 1024, 0, stream>>>(hist, histCount);
+        k_sort_scatter<<<sortBlocks, kSortBlock, 0, stream>>>(keysA, valsA, keysB, valsB, n, shift, hist, sortBlocks);
+        std::swap(keysA, keysB);
+        std::swap(valsA, valsB);
+    }
+    if (nInternal > 0)
+    {
+        k_karras<<<div_up(nInternal, 256), 256, 0, stream>>>(keysA, n, child, range, parent);
+        BUILD_CHECK(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)nInternal, stream));
+    }
+    else
+    {
+        int minus1 = -1;
+        BUILD_CHECK(cudaMemcpyAsync(parent, &minus1, sizeof(int), cudaMemcpyHostToDevice, stream));
+    }
+    k_refit<<<div_up(n, 256), 256, 0, stream>>>(n, valsA, triBox, child, parent, box, flag);
+    BUILD_CHECK(cudaGetLastError());
+
+    {
+        // collapse, one level per launch
+        int2 root = make_int2(n > 1 ? 0 : ~0, 0);
+        int init[4] = {1, 0, 0, 0};   // nodeCounter, triCounter, nextCount, error
+        BUILD_CHECK(cudaMemcpyAsync(workA, &root, sizeof(int2), cudaMemcpyHostToDevice, stream));
+        BUILD_CHECK(cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        CollapseArgs a;
+        a.n = n;
+        a.child = child;
+        a.range = range;
+        a.box = box;
+        a.vals = valsA;
+        a.pos = dPos;
+        a.idx = dIdx;
+        a.nodes = out.nodes;
+        a.tris = out.tris;
+        a.nodeCounter = counters + 0;
+        a.triCounter = counters + 1;
+        a.nodeCapacity = nodeCapacity;
+        a.error = counters + 3;
+        int workCount = 1;
+        while (workCount > 0)
+        {
+            BUILD_CHECK(cudaMemsetAsync(counters + 2, 0, sizeof(int), stream));
+            k_collapse<<<div_up(workCount, 128), 128, 0, stream>>>(a, workA, workCount, workB, counters + 2);
+            BUILD_CHECK(cudaGetLastError());
+            BUILD_CHECK(cudaMemcpyAsync(hostCounters, counters, sizeof(hostCounters), cudaMemcpyDeviceToHost, stream));
+            BUILD_CHECK(cudaStreamSynchronize(stream));
+            ++levels;
+            if (hostCounters[3])
+            {
+                err = "BVH8 collapse exceeded its node capacity";
+                status = PRT_EINTERNAL;
+                goto done;
+            }
+            workCount = hostCounters[2];
+            std::swap(workA, workB);
+        }
+        out.nodeCount = hostCounters[0];
+        out.triCount = hostCounters[1];
+        out.levels = levels;
+        if (out.triCount != n)
+        {
+            err = "BVH8 collapse lost triangles";
+            status = PRT_EINTERNAL;
+            goto done;
+        }
+        if (levels > kStackMax)
+        {
+            err = "BVH8 is deeper than the traversal stack";
+            status = PRT_EINTERNAL;
+            goto done;
+        }
+    }
+    BUILD_CHECK(cudaEventRecord(ev1, stream));
+    BUILD_CHECK(cudaEventSynchronize(ev1));
+    if (info)
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        info->buildMs = ms;
+        info->nodeCount = out.nodeCount;
+        info->levels = levels;
+    }
+
+done:
+    cudaFree(triBox);
+    cudaFree(partial);
+    cudaFree(cbounds);
+    cudaFree(keysA);
+    cudaFree(keysB);
+    cudaFree(valsA);
+    cudaFree(valsB);
+    cudaFree(hist);
+    cudaFree(child);
+    cudaFree(range);
+    cudaFree(parent);
+    cudaFree(flag);
+    cudaFree(box);
+    cudaFree(workA);
+    cudaFree(workB);
+    cudaFree(counters);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (status != PRT_OK) out.release();
+    return status;
+}
+
+} // namespace prt_b200

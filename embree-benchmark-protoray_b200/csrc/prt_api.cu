@@ -1,0 +1,1061 @@
+// C ABI of the B200 diffuse path tracer (declared in include/prt_b200.h).
+//
+// Host-side runtime: context and device memory, .mesh loading, camera set-up,
+// CUDA-graph capture of whole render calls, batched rendering, the path-replay
+// adjoint and the launch-configuration autotuner.  All device work runs on the
+// context's own stream; the only host synchronisations are at the end of a
+// render call (ray-count read-back) and in the build's level loop.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "prt_internal.h"
+
+using namespace prt_b200;
+
+namespace prt_b200 {
+int replay_max_depth();
+}
+
+struct prt_ctx
+{
+    int device = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::string name;
+
+    // mesh
+    float* dPos = nullptr;
+    int* dIdx = nullptr;
+    int nv = 0, nt = 0;
+    bool haveMesh = false;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    float* dAlbedo = nullptr;
+    float sky = 1.0f;
+
+    // acceleration structure
+    Bvh8Device bvh;
+    bool built = false;
+
+    // camera / frame
+    prt_camera cam{};
+    bool haveCamera = false;
+    int W = 0, H = 0;
+    float4* dAccum = nullptr;
+
+    // render state
+    int* dPass = nullptr;                 // device pass counter
+    unsigned long long* dRays = nullptr;  // rays of the current call
+    int* dCounts = nullptr;               // [kMaxDepthCap + 2]
+    int* dFetch = nullptr;                // [kMaxDepthCap + 2]
+    PathRec* q[2] = {nullptr, nullptr};
+    float* thr[2] = {nullptr, nullptr};
+    long long queueCap = 0;
+    bool queueThr = false;
+
+    // query scratch
+    RayRec* dRay = nullptr;
+    HitRec* dHit = nullptr;
+    float* dPNg = nullptr;
+
+    // batch scratch
+    BatchReq* dReqs = nullptr;
+    int reqCap = 0;
+
+    LaunchCfg cfg;
+    long long launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    struct GraphEntry
+    {
+        std::string key;
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;
+    };
+    std::vector<GraphEntry> graphs;
+
+    ~prt_ctx();
+};
+
+namespace {
+
+constexpr int kMaxDepthCap = 64;
+
+int fail(prt_ctx* c, int status, const std::string& msg)
+{
+    if (c) c->err = msg;
+    return status;
+}
+
+#define CK(call)                                                                                                 \
+    do                                                                                                           \
+    {                                                                                                            \
+        cudaError_t e_ = (call);                                                                                 \
+        if (e_ != cudaSuccess)                                                                                   \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA,                          \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                                     \
+    } while (0)
+
+bool is_device_ptr(const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+void clear_graphs(prt_ctx* ctx)
+{
+    for (auto& g : ctx->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    ctx->graphs.clear();
+}
+
+SceneDev scene_dev(const prt_ctx* ctx)
+{
+    SceneDev s;
+    s.nodes = ctx->bvh.nodes;
+    s.tris = ctx->bvh.tris;
+    s.albedo = ctx->dAlbedo;
+    s.triCount = ctx->nt;
+    s.hasRoot = ctx->bvh.nodeCount > 0 ? 1 : 0;
+    return s;
+}
+
+CameraDev camera_dev(const prt_camera& c, int W, int H)
+{
+    CameraDev d;
+    d.origin = make_float3(c.origin[0], c.origin[1], c.origin[2]);
+    d.basisU = make_float3(c.basisU[0], c.basisU[1], c.basisU[2]);
+    d.basisV = make_float3(c.basisV[0], c.basisV[1], c.basisV[2]);
+    d.imageO = make_float3(c.imageO[0], c.imageO[1], c.imageO[2]);
+    d.imageDx = make_float3(c.imageDx[0], c.imageDx[1], c.imageDx[2]);
+    d.imageDy = make_float3(c.imageDy[0], c.imageDy[1], c.imageDy[2]);
+    d.lensRadius = c.lensRadius;
+    d.focalDistance = c.focalDistance;
+    d.invW = 1.0f / (float)W;
+    d.invH = 1.0f / (float)H;
+    d.width = W;
+    d.height = H;
+    return d;
+}
+
+__global__ void k_check_indices(const int* idx, long long n3, int nv, int* bad)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    {
+        int v = idx[i];
+        if (v < 0 || v >= nv) atomicAdd(bad, 1);
+    }
+}
+
+int ensure_queues(prt_ctx* ctx, long long paths, bool withThr)
+{
+    if (paths <= ctx->queueCap && (!withThr || ctx->queueThr)) return PRT_OK;
+    for (int i = 0; i < 2; ++i)
+    {
+        cudaFree(ctx->q[i]);
+        cudaFree(ctx->thr[i]);
+        ctx->q[i] = nullptr;
+        ctx->thr[i] = nullptr;
+    }
+    clear_graphs(ctx);
+    long long cap = std::max(paths, ctx->queueCap);
+    for (int i = 0; i < 2; ++i)
+    {
+        CK(cudaMalloc(&ctx->q[i], sizeof(PathRec) * (size_t)cap));
+        if (withThr || ctx->queueThr) CK(cudaMalloc(&ctx->thr[i], sizeof(float) * (size_t)cap));
+    }
+    ctx->queueCap = cap;
+    ctx->queueThr = withThr || ctx->queueThr;
+    return PRT_OK;
+}
+
+long long default_paths_per_wave(const prt_ctx* ctx)
+{
+    // enough paths in flight to keep every SM busy down to the last bounce
+    return std::max<long long>(1 << 21, (long long)ctx->numSMs * 8192);
+}
+
+// Throughput after `depth` non-final bounces with the constant albedo 0.8,
+// multiplied in float as the reference does (render/diffuse_renderer_cuda.cu:182,209).
+float const_throughput(int depth)
+{
+    float t = 1.0f;
+    for (int d = 0; d < depth; ++d) t *= 0.8f;
+    return t;
+}
+
+int passes_per_wave(const prt_ctx* ctx, int spp)
+{
+    const long long perPass = (long long)((ctx->W + 7) / 8) * ((ctx->H + 7) / 8) * 64;
+    long long ppw = ctx->cfg.pathsPerWave > 0 ? ctx->cfg.pathsPerWave : default_paths_per_wave(ctx);
+    return (int)std::max<long long>(1, std::min<long long>(spp, ppw / perPass));
+}
+
+// Records every device operation of one render call on ctx->stream (the
+// queues are allocated beforehand: no allocation happens during capture).
+int record_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, int& launches)
+{
+    const int W = ctx->W, H = ctx->H;
+    const int tilesX = (W + 7) / 8, tilesY = (H + 7) / 8;
+    const long long perPass = (long long)tilesX * tilesY * 64;
+    const int passesPerWave = passes_per_wave(ctx, spp);
+    const bool albedo = ctx->dAlbedo != nullptr;
+    if (ctx->queueCap < (long long)passesPerWave * perPass || (albedo && !ctx->queueThr))
+        return fail(ctx, PRT_EINTERNAL, "path queues too small");
+
+    launches = 0;
+    if (!accumulate) CK(cudaMemsetAsync(ctx->dAccum, 0, sizeof(float4) * (size_t)W * H, ctx->stream));
+    CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+    WaveArgs a;
+    a.scene = scene_dev(ctx);
+    a.cam = camera_dev(ctx->cam, W, H);
+    a.accum = ctx->dAccum;
+    a.counts = ctx->dCounts;
+    a.fetch = ctx->dFetch;
+    a.rays = ctx->dRays;
+    a.passBase = ctx->dPass;
+    a.tilesX = tilesX;
+    a.tilesY = tilesY;
+    a.maxDepth = maxDepth;
+    a.sky = ctx->sky;
+    for (int p0 = 0; p0 < spp; p0 += passesPerWave)
+    {
+        a.passOffset = p0;
+        a.passes = std::min(passesPerWave, spp - p0);
+        CK(cudaMemsetAsync(ctx->dCounts, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+        CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+        for (int d = 0; d <= maxDepth; ++d)
+        {
+            a.qin = d == 0 ? nullptr : ctx->q[(d - 1) & 1];
+            a.qout = ctx->q[d & 1];
+            a.thrIn = albedo && d > 0 ? ctx->thr[(d - 1) & 1] : nullptr;
+            a.thrOut = albedo ? ctx->thr[d & 1] : nullptr;
+            a.thrConst = const_throughput(d);
+            launches += launch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
+        }
+    }
+    launches += launch_advance_pass(ctx->dPass, spp, ctx->stream);
+    CK(cudaGetLastError());
+    return PRT_OK;
+}
+
+int run_graph(prt_ctx* ctx, const std::string& key, const std::function<int(int&)>& record, int& launches)
+{
+    for (auto& g : ctx->graphs)
+        if (g.key == key)
+        {
+            CK(cudaGraphLaunch(g.exec, ctx->stream));
+            launches = g.launches;
+            return PRT_OK;
+        }
+    if (ctx->graphs.size() >= 16) clear_graphs(ctx);
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int st = record(launches);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st != PRT_OK)
+    {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(ctx, PRT_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, PRT_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    prt_ctx::GraphEntry ge;
+    ge.key = key;
+    ge.exec = exec;
+    ge.launches = launches;
+    ctx->graphs.push_back(ge);
+    CK(cudaGraphLaunch(exec, ctx->stream));
+    return PRT_OK;
+}
+
+int finish_stats(prt_ctx* ctx, prt_render_stats* stats, int passes)
+{
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    unsigned long long rays = 0;
+    CK(cudaMemcpy(&rays, ctx->dRays, sizeof(rays), cudaMemcpyDeviceToHost));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (stats)
+    {
+        stats->rays = (long long)rays;
+        stats->ms = ms;
+        stats->mray = ms > 0 ? (double)rays / 1e6 / (ms / 1e3) : 0.0;
+        stats->passes = passes;
+    }
+    return PRT_OK;
+}
+
+int check_ready(prt_ctx* ctx, bool needFrame)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (!ctx->built) return fail(ctx, PRT_ESTATE, "acceleration structure not built (prt_build_accel)");
+    if (needFrame && !ctx->dAccum) return fail(ctx, PRT_ESTATE, "frame not initialised (prt_init_frame)");
+    if (needFrame && !ctx->haveCamera) return fail(ctx, PRT_ESTATE, "camera not set (prt_set_camera)");
+    return PRT_OK;
+}
+
+// --- .mesh blob reader (geometry/triangle_mesh.cpp:305-320, sys/blob.h:26-38) ---
+struct MeshFile
+{
+    std::vector<int> idx;
+    std::vector<float> pos;
+    float lo[3], hi[3];
+};
+
+int read_mesh_file(prt_ctx* ctx, const char* path, MeshFile& m)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return fail(ctx, PRT_EIO, std::string("cannot open ") + path);
+    f.seekg(0, std::ios::end);
+    long long size = f.tellg();
+    f.seekg(0);
+    std::vector<char> data((size_t)std::max<long long>(size, 0));
+    if (size > 0) f.read(data.data(), size);
+    if (!f) return fail(ctx, PRT_EIO, std::string("read error: ") + path);
+    size_t off = 0;
+    auto take = [&](void* dst, size_t n) {
+        if (off + n > data.size()) return false;
+        std::memcpy(dst, data.data() + off, n);
+        off += n;
+        return true;
+    };
+    int id = 0;
+    if (!take(&id, 4)) return fail(ctx, PRT_EIO, "unexpected end of stream");
+    if (id != 0x04df8666) return fail(ctx, PRT_EIO, std::string("file has wrong blob ID: ") + path);
+    float b[6];
+    int tri = 0, vert = 0;
+    unsigned char hasN = 0, hasT = 0;
+    if (!take(b, 24) || !take(&tri, 4) || !take(&vert, 4) || !take(&hasN, 1) || !take(&hasT, 1))
+        return fail(ctx, PRT_EIO, "unexpected end of stream");
+    if (tri < 0 || vert < 0) return fail(ctx, PRT_EIO, "negative element count");
+    int stride = 3 + (hasN ? 3 : 0) + (hasT ? 2 : 0);
+    m.idx.resize(3 * (size_t)tri);
+    std::vector<int> mat((size_t)tri);
+    std::vector<float> attrs((size_t)vert * stride);
+    if (!take(m.idx.data(), 12 * (size_t)tri) || !take(mat.data(), 4 * (size_t)tri) ||
+        !take(attrs.data(), 4 * attrs.size()))
+        return fail(ctx, PRT_EIO, "unexpected end of stream");
+    int nnames = 0;
+    if (!take(&nnames, 4) || nnames < 0) return fail(ctx, PRT_EIO, "unexpected end of stream");
+    for (int i = 0; i < nnames; ++i)
+    {
+        int len = 0;
+        if (!take(&len, 4) || len < 0 || off + (size_t)len > data.size())
+            return fail(ctx, PRT_EIO, "unexpected end of stream");
+        off += (size_t)len;
+    }
+    m.pos.resize(3 * (size_t)vert);
+    for (int v = 0; v < vert; ++v)
+        for (int k = 0; k < 3; ++k) m.pos[3 * (size_t)v + k] = attrs[(size_t)v * stride + k];
+    for (int k = 0; k < 3; ++k)
+    {
+        m.lo[k] = b[k];
+        m.hi[k] = b[3 + k];
+    }
+    return PRT_OK;
+}
+
+} // namespace
+
+prt_ctx::~prt_ctx()
+{
+    cudaSetDevice(device);
+    clear_graphs(this);
+    bvh.release();
+    cudaFree(dPos);
+    cudaFree(dIdx);
+    cudaFree(dAlbedo);
+    cudaFree(dAccum);
+    cudaFree(dPass);
+    cudaFree(dRays);
+    cudaFree(dCounts);
+    cudaFree(dFetch);
+    for (int i = 0; i < 2; ++i)
+    {
+        cudaFree(q[i]);
+        cudaFree(thr[i]);
+    }
+    cudaFree(dRay);
+    cudaFree(dHit);
+    cudaFree(dPNg);
+    cudaFree(dReqs);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+extern "C" {
+
+int prt_create(int device, prt_ctx** out)
+{
+    if (!out) return PRT_EINVAL;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return PRT_ECUDA;
+    if (device < 0 || device >= count) return PRT_EINVAL;
+    std::unique_ptr<prt_ctx> c(new prt_ctx);
+    prt_ctx* ctx = c.get();
+    ctx->device = device;
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    ctx->numSMs = prop.multiProcessorCount;
+    ctx->name = prop.name;
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ctx->ev0));
+    CK(cudaEventCreate(&ctx->ev1));
+    CK(cudaMalloc(&ctx->dPass, sizeof(int)));
+    CK(cudaMemset(ctx->dPass, 0, sizeof(int)));
+    CK(cudaMalloc(&ctx->dRays, sizeof(unsigned long long)));
+    CK(cudaMalloc(&ctx->dCounts, sizeof(int) * (kMaxDepthCap + 2)));
+    CK(cudaMalloc(&ctx->dFetch, sizeof(int) * (kMaxDepthCap + 2)));
+    CK(cudaMalloc(&ctx->dRay, sizeof(RayRec)));
+    CK(cudaMalloc(&ctx->dHit, sizeof(HitRec)));
+    CK(cudaMalloc(&ctx->dPNg, sizeof(float) * 6));
+    *out = c.release();
+    return PRT_OK;
+}
+
+int prt_destroy(prt_ctx* ctx)
+{
+    if (!ctx) return PRT_EINVAL;
+    delete ctx;
+    return PRT_OK;
+}
+
+const char* prt_last_error(const prt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int prt_get_info(prt_ctx* ctx, char* buf, int len)
+{
+    if (!ctx || !buf || len <= 0) return PRT_EINVAL;
+    std::snprintf(buf, (size_t)len, "%s", ctx->name.c_str());
+    return PRT_OK;
+}
+
+long long prt_launch_count(prt_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int prt_load_mesh(prt_ctx* ctx, const int* indices, int triCount, const float* positions, int vertCount)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (triCount < 0 || vertCount < 0) return fail(ctx, PRT_EINVAL, "negative element count");
+    if ((triCount > 0 && !indices) || (vertCount > 0 && !positions)) return fail(ctx, PRT_EINVAL, "null mesh array");
+    CK(cudaSetDevice(ctx->device));
+    clear_graphs(ctx);
+    ctx->bvh.release();
+    ctx->built = false;
+    cudaFree(ctx->dPos);
+    cudaFree(ctx->dIdx);
+    cudaFree(ctx->dAlbedo);
+    ctx->dPos = nullptr;
+    ctx->dIdx = nullptr;
+    ctx->dAlbedo = nullptr;
+    ctx->haveMesh = false;
+    CK(cudaMalloc(&ctx->dPos, sizeof(float) * 3 * (size_t)std::max(vertCount, 1)));
+    CK(cudaMalloc(&ctx->dIdx, sizeof(int) * 3 * (size_t)std::max(triCount, 1)));
+    if (vertCount)
+        CK(cudaMemcpyAsync(ctx->dPos, positions, sizeof(float) * 3 * (size_t)vertCount, cudaMemcpyDefault, ctx->stream));
+    if (triCount)
+        CK(cudaMemcpyAsync(ctx->dIdx, indices, sizeof(int) * 3 * (size_t)triCount, cudaMemcpyDefault, ctx->stream));
+    // every index must name a vertex: the kernels gather positions unchecked
+    int* dBad = nullptr;
+    CK(cudaMalloc(&dBad, sizeof(int)));
+    CK(cudaMemsetAsync(dBad, 0, sizeof(int), ctx->stream));
+    if (triCount)
+    {
+        k_check_indices<<<256, 256, 0, ctx->stream>>>(ctx->dIdx, 3LL * triCount, vertCount, dBad);
+        ctx->launches++;
+    }
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, dBad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dBad);
+    if (bad) return fail(ctx, PRT_EINVAL, "triangle index out of range");
+    // bounds (host copy of the positions when they came from the host)
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (vertCount)
+    {
+        std::vector<float> hp(3 * (size_t)vertCount);
+        CK(cudaMemcpy(hp.data(), ctx->dPos, sizeof(float) * hp.size(), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < 3; ++k) { lo[k] = hp[k]; hi[k] = hp[k]; }
+        for (int v = 1; v < vertCount; ++v)
+            for (int k = 0; k < 3; ++k)
+            {
+                lo[k] = std::min(lo[k], hp[3 * (size_t)v + k]);
+                hi[k] = std::max(hi[k], hp[3 * (size_t)v + k]);
+            }
+    }
+    std::memcpy(ctx->lo, lo, sizeof(lo));
+    std::memcpy(ctx->hi, hi, sizeof(hi));
+    ctx->nt = triCount;
+    ctx->nv = vertCount;
+    ctx->haveMesh = true;
+    return PRT_OK;
+}
+
+int prt_load_mesh_file(prt_ctx* ctx, const char* path, float boundsLo[3], float boundsHi[3])
+{
+    if (!ctx || !path) return PRT_EINVAL;
+    MeshFile m;
+    int st = read_mesh_file(ctx, path, m);
+    if (st != PRT_OK) return st;
+    st = prt_load_mesh(ctx, m.idx.data(), (int)(m.idx.size() / 3), m.pos.data(), (int)(m.pos.size() / 3));
+    if (st != PRT_OK) return st;
+    // the stored box is the scene bounds of the reference (TriangleMesh::bounds)
+    std::memcpy(ctx->lo, m.lo, sizeof(m.lo));
+    std::memcpy(ctx->hi, m.hi, sizeof(m.hi));
+    if (boundsLo) std::memcpy(boundsLo, m.lo, sizeof(m.lo));
+    if (boundsHi) std::memcpy(boundsHi, m.hi, sizeof(m.hi));
+    return PRT_OK;
+}
+
+int prt_get_scene_bounds(prt_ctx* ctx, float lo[3], float hi[3])
+{
+    if (!ctx || !lo || !hi) return PRT_EINVAL;
+    if (!ctx->haveMesh) return fail(ctx, PRT_ESTATE, "no scene loaded");
+    std::memcpy(lo, ctx->lo, sizeof(ctx->lo));
+    std::memcpy(hi, ctx->hi, sizeof(ctx->hi));
+    return PRT_OK;
+}
+
+int prt_set_albedo(prt_ctx* ctx, const float* albedo, int triCount)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (!ctx->haveMesh) return fail(ctx, PRT_ESTATE, "no scene loaded");
+    CK(cudaSetDevice(ctx->device));
+    clear_graphs(ctx);
+    if (!albedo)
+    {
+        cudaFree(ctx->dAlbedo);
+        ctx->dAlbedo = nullptr;
+        return PRT_OK;
+    }
+    if (triCount != ctx->nt) return fail(ctx, PRT_EINVAL, "albedo count differs from the triangle count");
+    if (!ctx->dAlbedo) CK(cudaMalloc(&ctx->dAlbedo, sizeof(float) * (size_t)std::max(ctx->nt, 1)));
+    if (ctx->nt)
+        CK(cudaMemcpyAsync(ctx->dAlbedo, albedo, sizeof(float) * (size_t)ctx->nt, cudaMemcpyDefault, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_set_sky(prt_ctx* ctx, float sky)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (!std::isfinite(sky)) return fail(ctx, PRT_EINVAL, "sky radiance must be finite");
+    ctx->sky = sky;
+    clear_graphs(ctx);
+    return PRT_OK;
+}
+
+int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (!ctx->haveMesh) return fail(ctx, PRT_ESTATE, "no scene loaded");
+    CK(cudaSetDevice(ctx->device));
+    clear_graphs(ctx);
+    ctx->built = false;
+    BuildInfo info;
+    std::string err;
+    int st = build_bvh8(ctx->dPos, ctx->nv, ctx->dIdx, ctx->nt, ctx->bvh, ctx->stream, err, &info);
+    if (st != PRT_OK) return fail(ctx, st, err);
+    ctx->built = true;
+    if (stats)
+    {
+        stats->buildMs = info.buildMs;
+        stats->buildMprim = info.buildMs > 0 ? (double)ctx->nt / 1e6 / (info.buildMs / 1e3) : 0.0;
+        stats->nodeCount = ctx->bvh.nodeCount;
+        stats->levels = ctx->bvh.levels;
+    }
+    return PRT_OK;
+}
+
+int prt_camera_from_view(const prt_view* v, int width, int height, prt_camera* cam)
+{
+    if (!v || !cam || width <= 0 || height <= 0) return PRT_EINVAL;
+    // Basis3f(one).rotateV(angleY).rotateU(angleX) (math/basis3.h:63-79) with
+    // rotate() of math/vec3.h:409-412, then PinholeCamera's image plane
+    // (camera/pinhole_camera.h:40-47), all in float in the reference's order.
+    struct V3 { float x, y, z; };
+    auto vadd = [](V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; };
+    auto vmul = [](V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; };
+    auto vdot = [](V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; };
+    auto vcross = [](V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; };
+    auto rotate = [&](V3 vec, V3 axis, float ang) {
+        float c = std::cos(ang), s = std::sin(ang);
+        return vadd(vadd(vmul(vec, c), vmul(vmul(axis, vdot(axis, vec)), 1.0f - c)), vmul(vcross(vec, axis), s));
+    };
+    V3 V0{0, 1, 0}, N0{0, 0, 1};
+    V3 N1 = rotate(N0, V0, v->angleY);
+    V3 U1 = vcross(V0, N1);
+    V3 V2 = rotate(V0, U1, v->angleX);
+    V3 N2 = vcross(U1, V2);
+    float aspect = (float)width / (float)height;
+    float hh = std::tan(0.5f * v->fovY);
+    float hw = hh * aspect;
+    auto basis = [&](float ax, float ay, float az) { return vadd(vadd(vmul(U1, ax), vmul(V2, ay)), vmul(N2, az)); };
+    V3 O = basis(-hw, hh, -1.0f);
+    V3 Dx = basis(2.0f * hw, 0.0f, 0.0f);
+    V3 Dy = basis(0.0f, (float)(-2.0 * (double)hh), 0.0f);
+    auto put = [](float* d, V3 a) { d[0] = a.x; d[1] = a.y; d[2] = a.z; };
+    cam->origin[0] = v->pos[0];
+    cam->origin[1] = v->pos[1];
+    cam->origin[2] = v->pos[2];
+    put(cam->basisU, U1);
+    put(cam->basisV, V2);
+    put(cam->imageO, O);
+    put(cam->imageDx, Dx);
+    put(cam->imageDy, Dy);
+    cam->lensRadius = v->radius;
+    cam->focalDistance = v->focus;
+    return PRT_OK;
+}
+
+int prt_set_camera(prt_ctx* ctx, const prt_camera* cam)
+{
+    if (!ctx || !cam) return PRT_EINVAL;
+    // captured render graphs bake the camera into their kernel arguments
+    if (!ctx->haveCamera || std::memcmp(&ctx->cam, cam, sizeof(prt_camera)) != 0) clear_graphs(ctx);
+    ctx->cam = *cam;
+    ctx->haveCamera = true;
+    return PRT_OK;
+}
+
+int prt_init_frame(prt_ctx* ctx, int width, int height)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (width <= 0 || height <= 0 || (long long)width * height > (1LL << 28))
+        return fail(ctx, PRT_EINVAL, "invalid frame size");
+    CK(cudaSetDevice(ctx->device));
+    clear_graphs(ctx);
+    cudaFree(ctx->dAccum);
+    ctx->dAccum = nullptr;
+    CK(cudaMalloc(&ctx->dAccum, sizeof(float4) * (size_t)width * height));
+    ctx->W = width;
+    ctx->H = height;
+    return prt_clear(ctx);
+}
+
+int prt_clear(prt_ctx* ctx)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (!ctx->dAccum) return fail(ctx, PRT_ESTATE, "frame not initialised (prt_init_frame)");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemsetAsync(ctx->dAccum, 0, sizeof(float4) * (size_t)ctx->W * ctx->H, ctx->stream));
+    CK(cudaMemsetAsync(ctx->dPass, 0, sizeof(int), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_set_pass(prt_ctx* ctx, int pass)
+{
+    if (!ctx || pass < 0) return PRT_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->dPass, &pass, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_get_pass(prt_ctx* ctx, int* pass)
+{
+    if (!ctx || !pass) return PRT_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(pass, ctx->dPass, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_read_accum(prt_ctx* ctx, float* rgbw)
+{
+    if (!ctx || !rgbw) return PRT_EINVAL;
+    if (!ctx->dAccum) return fail(ctx, PRT_ESTATE, "frame not initialised (prt_init_frame)");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(rgbw, ctx->dAccum, sizeof(float4) * (size_t)ctx->W * ctx->H, cudaMemcpyDefault, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_read_ldr(prt_ctx* ctx, uint32_t* bgra)
+{
+    if (!ctx || !bgra) return PRT_EINVAL;
+    if (!ctx->dAccum) return fail(ctx, PRT_ESTATE, "frame not initialised (prt_init_frame)");
+    CK(cudaSetDevice(ctx->device));
+    size_t n = (size_t)ctx->W * ctx->H;
+    uint32_t* dOut = nullptr;
+    bool dev = is_device_ptr(bgra);
+    if (dev) dOut = bgra;
+    else CK(cudaMalloc(&dOut, sizeof(uint32_t) * n));
+    ctx->launches += launch_resolve_ldr(ctx->dAccum, dOut, (int)n, ctx->stream);
+    CK(cudaGetLastError());
+    if (!dev) CK(cudaMemcpyAsync(bgra, dOut, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (!dev) cudaFree(dOut);
+    return PRT_OK;
+}
+
+int prt_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, prt_render_stats* stats)
+{
+    int st = check_ready(ctx, true);
+    if (st != PRT_OK) return st;
+    if (spp < 0 || maxDepth < 0 || maxDepth > kMaxDepthCap) return fail(ctx, PRT_EINVAL, "invalid spp or maxDepth");
+    CK(cudaSetDevice(ctx->device));
+    if (spp > 0)
+    {
+        const long long perPass = (long long)((ctx->W + 7) / 8) * ((ctx->H + 7) / 8) * 64;
+        st = ensure_queues(ctx, (long long)passes_per_wave(ctx, spp) * perPass, ctx->dAlbedo != nullptr);
+        if (st != PRT_OK) return st;
+    }
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (spp > 0)
+    {
+        std::ostringstream key;
+        key << "render:" << spp << ":" << maxDepth << ":" << accumulate << ":" << ctx->cfg.block << ":"
+            << ctx->cfg.blocksPerSM << ":" << ctx->cfg.pathsPerWave;
+        int launches = 0;
+        st = run_graph(ctx, key.str(), [&](int& l) { return record_render(ctx, spp, maxDepth, accumulate, l); },
+                       launches);
+        if (st != PRT_OK) return st;
+        ctx->launches += launches;
+    }
+    else
+    {
+        CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+    }
+    return finish_stats(ctx, stats, spp);
+}
+
+int prt_query_ray(prt_ctx* ctx, const prt_ray* ray, prt_hit* hit, float p[3], float Ng[3])
+{
+    int st = check_ready(ctx, false);
+    if (st != PRT_OK) return st;
+    if (!ray || !hit) return fail(ctx, PRT_EINVAL, "null ray or hit");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->dRay, ray, sizeof(RayRec), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->launches += launch_query(scene_dev(ctx), ctx->dRay, ctx->dHit, ctx->dPNg, ctx->stream);
+    CK(cudaGetLastError());
+    float png[6];
+    CK(cudaMemcpyAsync(hit, ctx->dHit, sizeof(HitRec), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(png, ctx->dPNg, sizeof(png), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (hit->t >= 0.f)
+    {
+        if (p) std::memcpy(p, png, 12);
+        if (Ng) std::memcpy(Ng, png + 3, 12);
+    }
+    return PRT_OK;
+}
+
+int prt_intersect(prt_ctx* ctx, const prt_ray* rays, prt_hit* hits, int n, void* stream)
+{
+    int st = check_ready(ctx, false);
+    if (st != PRT_OK) return st;
+    if (n < 0 || (n > 0 && (!rays || !hits))) return fail(ctx, PRT_EINVAL, "invalid ray buffers");
+    if (n > 0 && (!is_device_ptr(rays) || !is_device_ptr(hits)))
+        return fail(ctx, PRT_EINVAL, "prt_intersect takes device pointers");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    ctx->launches += launch_intersect(scene_dev(ctx), (const RayRec*)rays, (HitRec*)hits, n, false, nullptr, s);
+    CK(cudaGetLastError());
+    if (!stream) CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_occluded(prt_ctx* ctx, const prt_ray* rays, float* out, int n, void* stream)
+{
+    int st = check_ready(ctx, false);
+    if (st != PRT_OK) return st;
+    if (n < 0 || (n > 0 && (!rays || !out))) return fail(ctx, PRT_EINVAL, "invalid ray buffers");
+    if (n > 0 && (!is_device_ptr(rays) || !is_device_ptr(out)))
+        return fail(ctx, PRT_EINVAL, "prt_occluded takes device pointers");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    ctx->launches += launch_intersect(scene_dev(ctx), (const RayRec*)rays, nullptr, n, true, out, s);
+    CK(cudaGetLastError());
+    if (!stream) CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_render_replay(prt_ctx* ctx, int pass0, int spp, int maxDepth, prt_render_stats* stats)
+{
+    int st = check_ready(ctx, true);
+    if (st != PRT_OK) return st;
+    if (pass0 < 0 || spp < 0 || maxDepth < 0 || maxDepth > replay_max_depth())
+        return fail(ctx, PRT_EINVAL, "invalid pass range or maxDepth (replay supports maxDepth <= 16)");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+    ctx->launches += launch_replay(scene_dev(ctx), camera_dev(ctx->cam, ctx->W, ctx->H), ctx->dAccum, pass0, spp,
+                                   maxDepth, ctx->sky, nullptr, nullptr, nullptr, ctx->dRays, false, ctx->stream);
+    CK(cudaGetLastError());
+    return finish_stats(ctx, stats, spp);
+}
+
+int prt_render_backward(prt_ctx* ctx, int pass0, int spp, int maxDepth, const float* dL_dsum, float* d_albedo,
+                        float* d_sky)
+{
+    int st = check_ready(ctx, true);
+    if (st != PRT_OK) return st;
+    if (!dL_dsum || !d_albedo || !d_sky) return fail(ctx, PRT_EINVAL, "null gradient buffer");
+    if (pass0 < 0 || spp < 0 || maxDepth < 0 || maxDepth > replay_max_depth())
+        return fail(ctx, PRT_EINVAL, "invalid pass range or maxDepth (replay supports maxDepth <= 16)");
+    CK(cudaSetDevice(ctx->device));
+    const size_t npix = (size_t)ctx->W * ctx->H;
+    const bool devL = is_device_ptr(dL_dsum), devA = is_device_ptr(d_albedo), devS = is_device_ptr(d_sky);
+    float* gL = nullptr;
+    float* gA = nullptr;
+    float* gS = nullptr;
+    if (devL) gL = const_cast<float*>(dL_dsum);
+    else
+    {
+        CK(cudaMalloc(&gL, sizeof(float) * 3 * npix));
+        CK(cudaMemcpyAsync(gL, dL_dsum, sizeof(float) * 3 * npix, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (devA) gA = d_albedo;
+    else CK(cudaMalloc(&gA, sizeof(float) * (size_t)std::max(ctx->nt, 1)));
+    if (devS) gS = d_sky;
+    else CK(cudaMalloc(&gS, sizeof(float)));
+    CK(cudaMemsetAsync(gA, 0, sizeof(float) * (size_t)ctx->nt, ctx->stream));
+    CK(cudaMemsetAsync(gS, 0, sizeof(float), ctx->stream));
+    ctx->launches += launch_replay(scene_dev(ctx), camera_dev(ctx->cam, ctx->W, ctx->H), ctx->dAccum, pass0, spp,
+                                   maxDepth, ctx->sky, gL, gA, gS, nullptr, true, ctx->stream);
+    CK(cudaGetLastError());
+    if (!devA) CK(cudaMemcpyAsync(d_albedo, gA, sizeof(float) * (size_t)ctx->nt, cudaMemcpyDeviceToHost, ctx->stream));
+    if (!devS) CK(cudaMemcpyAsync(d_sky, gS, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (!devL) cudaFree(gL);
+    if (!devA) cudaFree(gA);
+    if (!devS) cudaFree(gS);
+    return PRT_OK;
+}
+
+int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_stats* stats)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (n < 0 || n > 255 || (n > 0 && !reqs)) return fail(ctx, PRT_EINVAL, "batch size must be 0..255");
+    CK(cudaSetDevice(ctx->device));
+    std::vector<BatchReq> table((size_t)n);
+    std::vector<float4*> tmp((size_t)n, nullptr);
+    long long total = 0;
+    int maxDepth = 0;
+    std::ostringstream key;
+    key << "batch:" << n << ":" << ctx->cfg.block << ":" << ctx->cfg.blocksPerSM << ":" << ctx->cfg.pathsPerWave;
+    for (int r = 0; r < n; ++r)
+    {
+        const prt_request& q = reqs[r];
+        if (!q.scene || !q.scene->built) return fail(ctx, PRT_ESTATE, "batch request scene not built");
+        if (q.scene->device != ctx->device) return fail(ctx, PRT_EINVAL, "batch request scene on another device");
+        if (q.scene->dAlbedo) return fail(ctx, PRT_EINVAL, "batched rendering uses the constant albedo");
+        if (q.width <= 0 || q.height <= 0 || (long long)q.width * q.height > (1LL << 24) || q.spp < 0 ||
+            q.maxDepth < 0 || q.maxDepth > kMaxDepthCap || !q.accum)
+            return fail(ctx, PRT_EINVAL, "invalid batch request");
+        BatchReq& b = table[(size_t)r];
+        b.scene = scene_dev(q.scene);
+        b.cam = camera_dev(q.camera, q.width, q.height);
+        b.tilesX = (q.width + 7) / 8;
+        b.tilesY = (q.height + 7) / 8;
+        b.spp = q.spp;
+        b.maxDepth = q.maxDepth;
+        b.pathBegin = total;
+        total += (long long)b.tilesX * b.tilesY * 64 * q.spp;
+        maxDepth = std::max(maxDepth, q.maxDepth);
+        key << ":" << (const void*)q.scene << "," << q.width << "x" << q.height << "," << q.spp << "," << q.maxDepth
+            << "," << (const void*)q.accum;
+        for (int k = 0; k < 3; ++k)
+            key << "," << q.camera.origin[k] << "," << q.camera.imageO[k] << "," << q.camera.imageDx[k] << ","
+                << q.camera.imageDy[k] << "," << q.camera.basisU[k] << "," << q.camera.basisV[k];
+        key << "," << q.camera.lensRadius << "," << q.camera.focalDistance;
+    }
+    key << ":sky" << ctx->sky;
+    // device accumulation buffers (caller's device memory in place)
+    bool anyTmp = false;
+    for (int r = 0; r < n; ++r)
+    {
+        const prt_request& q = reqs[r];
+        size_t bytes = sizeof(float4) * (size_t)q.width * q.height;
+        if (is_device_ptr(q.accum)) table[(size_t)r].accum = (float4*)q.accum;
+        else
+        {
+            CK(cudaMalloc(&tmp[(size_t)r], bytes));
+            table[(size_t)r].accum = tmp[(size_t)r];
+            anyTmp = true;
+        }
+    }
+    if (anyTmp) key << ":tmp";   // temporary buffers change per call: do not reuse a graph
+    if (n > ctx->reqCap)
+    {
+        cudaFree(ctx->dReqs);
+        ctx->dReqs = nullptr;
+        CK(cudaMalloc(&ctx->dReqs, sizeof(BatchReq) * (size_t)n));
+        ctx->reqCap = n;
+        clear_graphs(ctx);
+    }
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (n > 0)
+        CK(cudaMemcpyAsync(ctx->dReqs, table.data(), sizeof(BatchReq) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    for (int r = 0; r < n; ++r)
+        CK(cudaMemsetAsync(table[(size_t)r].accum, 0, sizeof(float4) * (size_t)reqs[r].width * reqs[r].height,
+                           ctx->stream));
+    long long ppw = ctx->cfg.pathsPerWave > 0 ? ctx->cfg.pathsPerWave : default_paths_per_wave(ctx);
+    int st = ensure_queues(ctx, std::min<long long>(ppw, std::max<long long>(total, 1)), false);
+    if (st != PRT_OK) return st;
+    auto record = [&](int& launches) -> int {
+        launches = 0;
+        CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+        BatchArgs a;
+        a.reqs = ctx->dReqs;
+        a.nreq = n;
+        a.counts = ctx->dCounts;
+        a.fetch = ctx->dFetch;
+        a.rays = ctx->dRays;
+        a.maxDepth = maxDepth;
+        a.sky = ctx->sky;
+        for (long long w0 = 0; w0 < total; w0 += ppw)
+        {
+            a.waveBegin = w0;
+            a.waveEnd = std::min(total, w0 + ppw);
+            CK(cudaMemsetAsync(ctx->dCounts, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+            CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+            for (int d = 0; d <= maxDepth; ++d)
+            {
+                a.qin = d == 0 ? nullptr : ctx->q[(d - 1) & 1];
+                a.qout = ctx->q[d & 1];
+                launches += launch_batch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
+            }
+        }
+        CK(cudaGetLastError());
+        return PRT_OK;
+    };
+    int launches = 0;
+    if (n > 0 && total > 0)
+    {
+        st = run_graph(ctx, key.str(), record, launches);
+        if (st != PRT_OK) return st;
+        ctx->launches += launches;
+    }
+    else
+    {
+        CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+    }
+    st = finish_stats(ctx, stats, 0);
+    for (int r = 0; r < n; ++r)
+        if (tmp[(size_t)r])
+        {
+            CK(cudaMemcpy(reqs[r].accum, tmp[(size_t)r], sizeof(float4) * (size_t)reqs[r].width * reqs[r].height,
+                          cudaMemcpyDeviceToHost));
+            cudaFree(tmp[(size_t)r]);
+        }
+    if (anyTmp)
+    {
+        // graphs that captured the temporary buffers are stale now
+        auto& g = ctx->graphs;
+        for (auto it = g.begin(); it != g.end();)
+            if (it->key == key.str()) { cudaGraphExecDestroy(it->exec); it = g.erase(it); }
+            else ++it;
+    }
+    return st;
+}
+
+int prt_set_tune(prt_ctx* ctx, const prt_tune* t)
+{
+    if (!ctx || !t) return PRT_EINVAL;
+    if (t->blockSize < 32 || t->blockSize > 256 || (t->blockSize & 31) || t->blocksPerSM < 1 || t->blocksPerSM > 64 ||
+        t->pathsPerWave < 0)
+        return fail(ctx, PRT_EINVAL, "invalid launch configuration");
+    ctx->cfg.block = t->blockSize;
+    ctx->cfg.blocksPerSM = t->blocksPerSM;
+    ctx->cfg.pathsPerWave = t->pathsPerWave;
+    clear_graphs(ctx);
+    return PRT_OK;
+}
+
+int prt_get_tune(prt_ctx* ctx, prt_tune* t)
+{
+    if (!ctx || !t) return PRT_EINVAL;
+    t->blockSize = ctx->cfg.block;
+    t->blocksPerSM = ctx->cfg.blocksPerSM;
+    t->pathsPerWave = ctx->cfg.pathsPerWave;
+    t->mray = 0;
+    return PRT_OK;
+}
+
+int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
+{
+    int st = check_ready(ctx, true);
+    if (st != PRT_OK) return st;
+    if (spp <= 0) return fail(ctx, PRT_EINVAL, "autotune needs spp > 0");
+    CK(cudaSetDevice(ctx->device));
+    const long long perPass = (long long)((ctx->W + 7) / 8) * ((ctx->H + 7) / 8) * 64;
+    LaunchCfg saved = ctx->cfg;
+    LaunchCfg bestCfg = saved;
+    double bestMray = -1;
+    const int blocks[] = {64, 128, 256};
+    const int perSM[] = {2, 4, 8, 16};
+    const long long waves[] = {1, 2, 4};
+    for (int b : blocks)
+        for (int s : perSM)
+        {
+            if (b * s > 2048) continue;   // more threads than an SM can hold
+            for (long long wv : waves)
+            {
+                long long ppw = std::max<long long>(perPass * wv, 1 << 16);
+                ctx->cfg.block = b;
+                ctx->cfg.blocksPerSM = s;
+                ctx->cfg.pathsPerWave = (int)std::min<long long>(ppw, 1LL << 30);
+                prt_render_stats rs;
+                CK(cudaMemsetAsync(ctx->dPass, 0, sizeof(int), ctx->stream));
+                st = prt_render(ctx, spp, maxDepth, 0, &rs);
+                if (st != PRT_OK)
+                {
+                    ctx->cfg = saved;
+                    return st;
+                }
+                // second run: graph already instantiated
+                CK(cudaMemsetAsync(ctx->dPass, 0, sizeof(int), ctx->stream));
+                st = prt_render(ctx, spp, maxDepth, 0, &rs);
+                if (st != PRT_OK)
+                {
+                    ctx->cfg = saved;
+                    return st;
+                }
+                if (rs.mray > bestMray)
+                {
+                    bestMray = rs.mray;
+                    bestCfg = ctx->cfg;
+                }
+                clear_graphs(ctx);
+            }
+        }
+    ctx->cfg = bestCfg;
+    clear_graphs(ctx);
+    st = prt_clear(ctx);
+    if (st != PRT_OK) return st;
+    if (best)
+    {
+        best->blockSize = bestCfg.block;
+        best->blocksPerSM = bestCfg.blocksPerSM;
+        best->pathsPerWave = bestCfg.pathsPerWave;
+        best->mray = bestMray;
+    }
+    return PRT_OK;
+}
+
+} // extern "C"

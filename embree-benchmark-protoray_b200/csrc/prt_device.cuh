@@ -1,0 +1,463 @@
+// Device-side building blocks of the B200 diffuse path tracer: records, RNG,
+// camera, compressed 8-wide BVH node layout, watertight traversal and the
+// diffuse bounce.  Everything here is __device__ code included by the kernels.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace prt_b200 {
+
+// ---------------------------------------------------------------------------
+// Small float3 helpers.  Arithmetic that decides a path's trajectory uses the
+// explicitly rounded intrinsics so that every kernel that replays a path
+// (forward wavefront, megakernel, adjoint) computes bit-identical rays no
+// matter how the compiler fuses the surrounding code.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 add(float3 a, float3 b) { return f3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)); }
+__device__ __forceinline__ float3 sub(float3 a, float3 b) { return f3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+__device__ __forceinline__ float3 mul(float3 a, float s) { return f3(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)); }
+__device__ __forceinline__ float dot(float3 a, float3 b)
+{
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 cross(float3 a, float3 b)
+{
+    return f3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+              __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+              __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float3 normalize(float3 a)
+{
+    float l2 = dot(a, a);
+    float inv = __frcp_rn(__fsqrt_rn(l2));
+    return mul(a, inv);
+}
+// a + s*b, rounded after each operation
+__device__ __forceinline__ float3 madd(float3 a, float s, float3 b) { return add(a, mul(b, s)); }
+
+// ---------------------------------------------------------------------------
+// Records.  RayRec/HitRec keep the 32-byte / 16-byte layouts of the reference
+// GPU interface (core/ray_cuda.cuh:23-80): a miss is t < 0.
+// ---------------------------------------------------------------------------
+
+struct RayRec
+{
+    float ox, oy, oz, tnear;
+    float dx, dy, dz, tfar;
+};
+
+struct HitRec
+{
+    float t;
+    int primId;
+    float u, v;
+};
+
+// Wavefront path record (32 bytes, two 16-byte words):
+//   w0 = {org.xyz, pixel id (int bits)}, w1 = {dir.xyz, RNG state (uint bits)}
+struct PathRec
+{
+    float4 w0;
+    float4 w1;
+};
+
+// ---------------------------------------------------------------------------
+// RNG: Murmur3 mixing of (pixel, pass) then an LCG stream
+// (sampling/random_sampler.cuh:29-103 and sampling/random_sampler.h:44-73).
+// uint32 -> float rounds to nearest as the reference CPU code does
+// (math/math.h:179), so GPU and CPU draw identical sample values.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t murmur_mix(uint32_t h, uint32_t k)
+{
+    k *= 0xcc9e2d51u;
+    k = __funnelshift_l(k, k, 15);
+    k *= 0x1b873593u;
+    h ^= k;
+    h = __funnelshift_l(h, h, 13) * 5u + 0xe6546b64u;
+    return h;
+}
+
+__device__ __forceinline__ uint32_t murmur_fin(uint32_t h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ uint32_t rng_seed(int pass, int pixel)
+{
+    return murmur_fin(murmur_mix(murmur_mix(0u, (uint32_t)pixel), (uint32_t)pass));
+}
+
+__device__ __forceinline__ float rng_next(uint32_t& s)
+{
+    s = s * 1664525u + 1013904223u;
+    return __fmul_rn(__uint2float_rn(s), 0x1.0p-32f);
+}
+
+// ---------------------------------------------------------------------------
+// Camera (fields of ThinLensCameraCuda, camera/thin_lens_camera_cuda.h:23-30)
+// ---------------------------------------------------------------------------
+
+struct CameraDev
+{
+    float3 origin;
+    float3 basisU, basisV;
+    float3 imageO, imageDx, imageDy;
+    float lensRadius, focalDistance;
+    float invW, invH;
+    int width, height;
+};
+
+// Primary ray for pixel (x, y) of pass `pass`: pixel jitter and lens sample
+// are the first two 2D draws (render/renderer_single.h:112-119); the pinhole
+// camera is used when the lens radius is 0 (render/device_cpu_impl.cpp:86-97).
+__device__ __forceinline__ void camera_ray(const CameraDev& cam, int x, int y, uint32_t& rng, float3& org, float3& dir)
+{
+    float jx = rng_next(rng);
+    float jy = rng_next(rng);
+    float lx = rng_next(rng);
+    float ly = rng_next(rng);
+    float ix = __fmul_rn(__fadd_rn((float)x, jx), cam.invW);
+    float iy = __fmul_rn(__fadd_rn((float)y, jy), cam.invH);
+    float3 d = add(add(cam.imageO, mul(cam.imageDx, ix)), mul(cam.imageDy, iy));
+    if (cam.lensRadius == 0.0f)
+    {
+        org = cam.origin;
+        dir = normalize(d);
+    }
+    else
+    {
+        // uniformSampleDisk (sampling/shape_sampler.h:114-124)
+        float r = __fsqrt_rn(lx);
+        float s, c;
+        sincosf(__fmul_rn(2.0f * 3.14159265358979f, ly), &s, &c);
+        float dx = __fmul_rn(__fmul_rn(r, c), cam.lensRadius);
+        float dy = __fmul_rn(__fmul_rn(r, s), cam.lensRadius);
+        float3 begin = add(add(cam.origin, mul(cam.basisU, dx)), mul(cam.basisV, dy));
+        float3 end = add(cam.origin, mul(d, cam.focalDistance));
+        org = begin;
+        dir = normalize(sub(end, begin));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Compressed 8-wide BVH node (80 bytes = 5 x 16 B).
+//   q0 = {origin.xyz, exponents x|y|z (biased by 127, bytes 0..2) | imask << 24}
+//   q1 = {child node base, triangle base, meta[0..3], meta[4..7]}
+//   q2 = {qlo.x[0..3], qlo.x[4..7], qlo.y[0..3], qlo.y[4..7]}
+//   q3 = {qlo.z[0..3], qlo.z[4..7], qhi.x[0..3], qhi.x[4..7]}
+//   q4 = {qhi.y[0..3], qhi.y[4..7], qhi.z[0..3], qhi.z[4..7]}
+// A child box is origin + q * 2^e per axis (8-bit q).  meta per slot:
+//   0                       empty slot
+//   0x20 | (24 + slot)      internal child (stored at base + rank among
+//                           internal slots of lower index, imask bit = slot)
+//   unary(n) << 5 | offset  leaf with n in 1..3 triangles at triBase+offset
+// Triangles are stored in leaf order, 48 bytes each: {v0, primId}, {v1, 0},
+// {v2, 0}.
+// Slot s is given to the child that comes first for rays whose direction
+// octant is s; traversal pops hits in the order of (slot ^ (7 - octant)).
+// ---------------------------------------------------------------------------
+
+struct Bvh8Node
+{
+    uint4 q[5];
+};
+
+struct TriRec
+{
+    float4 v0, v1, v2;
+};
+
+struct SceneDev
+{
+    const Bvh8Node* nodes;
+    const TriRec* tris;
+    const float* albedo;   // per original triangle id, or nullptr (constant 0.8)
+    int triCount;
+    int hasRoot;           // 0 for an empty scene
+};
+
+// Per-ray constants for traversal.
+struct TravRay
+{
+    float3 org;
+    float3 dir;
+    float3 inv;
+    uint32_t octinv;   // 7 - octant of dir
+    int kx, ky, kz;    // watertight shear axes
+    float Sx, Sy, Sz;
+};
+
+__device__ __forceinline__ void trav_setup(TravRay& r, float3 org, float3 dir)
+{
+    r.org = org;
+    r.dir = dir;
+    const float tiny = 1e-30f;
+    r.inv.x = 1.0f / (fabsf(dir.x) > tiny ? dir.x : copysignf(tiny, dir.x));
+    r.inv.y = 1.0f / (fabsf(dir.y) > tiny ? dir.y : copysignf(tiny, dir.y));
+    r.inv.z = 1.0f / (fabsf(dir.z) > tiny ? dir.z : copysignf(tiny, dir.z));
+    uint32_t oct = (dir.x < 0.f ? 1u : 0u) | (dir.y < 0.f ? 2u : 0u) | (dir.z < 0.f ? 4u : 0u);
+    r.octinv = 7u - oct;
+    float ax = fabsf(dir.x), ay = fabsf(dir.y), az = fabsf(dir.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    float dkz = kz == 0 ? dir.x : (kz == 1 ? dir.y : dir.z);
+    if (dkz < 0.f) { int t = kx; kx = ky; ky = t; }
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    float dkx = kx == 0 ? dir.x : (kx == 1 ? dir.y : dir.z);
+    float dky = ky == 0 ? dir.x : (ky == 1 ? dir.y : dir.z);
+    r.Sx = dkx / dkz;
+    r.Sy = dky / dkz;
+    r.Sz = 1.0f / dkz;
+}
+
+__device__ __forceinline__ float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2(1) 2013).
+// Accepts t in (tnear, tbest) — or t == tbest with a lower primitive id, so
+// that exact ties resolve the same way in every traversal order.  On a hit
+// returns true and sets t (and the barycentrics b1 -> u, b2 -> v, the
+// reference's convention, geometry/triangle_mesh.cpp:69-71).
+__device__ __forceinline__ bool tri_test(const TravRay& r, float3 v0, float3 v1, float3 v2, float tnear, float tbest,
+                                         int prim, int bestPrim, float& t, float& u, float& v)
+{
+    float3 A = sub(v0, r.org), B = sub(v1, r.org), C = sub(v2, r.org);
+    float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
+    float Ax = comp(A, r.kx) - r.Sx * Akz, Ay = comp(A, r.ky) - r.Sy * Akz;
+    float Bx = comp(B, r.kx) - r.Sx * Bkz, By = comp(B, r.ky) - r.Sy * Bkz;
+    float Cx = comp(C, r.kx) - r.Sx * Ckz, Cy = comp(C, r.ky) - r.Sy * Ckz;
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f)
+    {
+        // edge case: recompute the edge functions in double precision
+        double CxBy = (double)Cx * (double)By, CyBx = (double)Cy * (double)Bx;
+        U = (float)(CxBy - CyBx);
+        double AxCy = (double)Ax * (double)Cy, AyCx = (double)Ay * (double)Cx;
+        V = (float)(AxCy - AyCx);
+        double BxAy = (double)Bx * (double)Ay, ByAx = (double)By * (double)Ax;
+        W = (float)(BxAy - ByAx);
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+    float det = U + V + W;
+    if (det == 0.f) return false;
+    float T = U * (r.Sz * Akz) + V * (r.Sz * Bkz) + W * (r.Sz * Ckz);
+    // sign-aware range check without dividing
+    uint32_t sgn = __float_as_uint(det) & 0x80000000u;
+    float Ts = __uint_as_float(__float_as_uint(T) ^ sgn);
+    float dets = fabsf(det);
+    if (!(Ts > tnear * dets) || Ts > tbest * dets) return false;
+    float rcp = 1.0f / det;
+    float tt = T * rcp;
+    if (!(tt > tnear)) return false;
+    if (tt > tbest || (tt == tbest && prim >= bestPrim)) return false;
+    t = tt;
+    u = V * rcp;
+    v = W * rcp;
+    return true;
+}
+
+// Byte j of x as a float, exactly: 2^23 + byte built with a byte permute,
+// minus 2^23 (avoids the slower integer-to-float conversion).
+__device__ __forceinline__ float byte_f(uint32_t x, int j)
+{
+    return __uint_as_float(__byte_perm(x, 0x4b000000u, 0x7440u + (uint32_t)j)) - 8388608.0f;
+}
+
+// Intersection of the ray with the 8 child boxes of a node.  Returns the hit
+// mask: bits 24..31 internal children (traversal order), bits 0..23 triangles
+// relative to the node's triangle base.
+__device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, float tnear, float tfar)
+{
+    float px = __uint_as_float(q[0].x), py = __uint_as_float(q[0].y), pz = __uint_as_float(q[0].z);
+    uint32_t e = q[0].w;
+    float sx = __uint_as_float((e & 0xffu) << 23);
+    float sy = __uint_as_float(((e >> 8) & 0xffu) << 23);
+    float sz = __uint_as_float(((e >> 16) & 0xffu) << 23);
+    float aix = sx * r.inv.x, aiy = sy * r.inv.y, aiz = sz * r.inv.z;
+    float aox = (px - r.org.x) * r.inv.x, aoy = (py - r.org.y) * r.inv.y, aoz = (pz - r.org.z) * r.inv.z;
+    // For a negative direction component the far plane is the low plane:
+    // select per axis which byte array feeds the near / far distance.
+    bool nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
+    uint32_t loX[2] = {q[2].x, q[2].y}, loY[2] = {q[2].z, q[2].w}, loZ[2] = {q[3].x, q[3].y};
+    uint32_t hiX[2] = {q[3].z, q[3].w}, hiY[2] = {q[4].x, q[4].y}, hiZ[2] = {q[4].z, q[4].w};
+    uint32_t meta[2] = {q[1].z, q[1].w};
+    uint32_t hits = 0;
+    const float tfarp = tfar * 1.0000004f;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+    {
+        uint32_t nearX = nx ? hiX[h] : loX[h], farX = nx ? loX[h] : hiX[h];
+        uint32_t nearY = ny ? hiY[h] : loY[h], farY = ny ? loY[h] : hiY[h];
+        uint32_t nearZ = nz ? hiZ[h] : loZ[h], farZ = nz ? loZ[h] : hiZ[h];
+        uint32_t m4 = meta[h];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            uint32_t m = (m4 >> (8 * j)) & 0xffu;
+            float tnx = fmaf(byte_f(nearX, j), aix, aox);
+            float tny = fmaf(byte_f(nearY, j), aiy, aoy);
+            float tnz = fmaf(byte_f(nearZ, j), aiz, aoz);
+            float tfx = fmaf(byte_f(farX, j), aix, aox);
+            float tfy = fmaf(byte_f(farY, j), aiy, aoy);
+            float tfz = fmaf(byte_f(farZ, j), aiz, aoz);
+            float t0 = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tnear));
+            float t1 = fminf(fminf(tfx, tfy), fminf(tfz, tfarp));
+            bool hit = (m != 0u) && (t0 * 0.9999996f <= t1 * 1.0000004f);
+            if (hit)
+            {
+                uint32_t low = m & 0x1fu;
+                if (low >= 24u)
+                    hits |= 1u << (24u + ((low - 24u) ^ r.octinv));
+                else
+                    hits |= (m >> 5) << low;
+            }
+        }
+    }
+    return hits;
+}
+
+// Traversal stack: the first kShared entries of each thread live in shared
+// memory (one column per thread), deeper entries spill to local memory.
+constexpr int kShared = 8;
+constexpr int kLocal = 56;
+constexpr int kStackMax = kShared + kLocal;
+
+struct TravStack
+{
+    uint2* sh;         // shared base for this thread: sh[i * stride]
+    int stride;
+    uint2 loc[kLocal];
+    int sp;
+    bool overflow;
+
+    __device__ __forceinline__ void push(uint2 v)
+    {
+        if (sp < kShared) sh[sp * stride] = v;
+        else if (sp < kStackMax) loc[sp - kShared] = v;
+        else { overflow = true; return; }
+        ++sp;
+    }
+    __device__ __forceinline__ uint2 pop()
+    {
+        --sp;
+        return sp < kShared ? sh[sp * stride] : loc[sp - kShared];
+    }
+};
+
+// Closest hit (anyHit = false) or any hit (anyHit = true) over (tnear, tfar].
+// Returns the leaf-order triangle index of the hit (or -1), with t/u/v/prim.
+template <bool anyHit>
+__device__ __forceinline__ int traverse(const SceneDev& sc, const TravRay& r, float tnear, float tfar, TravStack& st,
+                                        float& tHit, int& primHit, float& uHit, float& vHit, int* nodeCount = nullptr)
+{
+    int triHit = -1;
+    primHit = 0x7fffffff;
+    tHit = tfar;
+    uHit = 0.f;
+    vHit = 0.f;
+    if (!sc.hasRoot) return -1;
+    st.sp = 0;
+    // root group: one internal "child" at base 0
+    uint2 ng = make_uint2(0u, 0x80000000u);
+    for (;;)
+    {
+        // ng holds at least one node bit here
+        uint32_t b = 31u - __clz(ng.y & 0xff000000u);
+        ng.y &= ~(1u << b);
+        uint32_t slot = (b - 24u) ^ r.octinv;
+        uint32_t rel = __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
+        uint32_t nodeIdx = ng.x + rel;
+        if (ng.y & 0xff000000u) st.push(ng);
+        const uint4* qp = reinterpret_cast<const uint4*>(sc.nodes + nodeIdx);
+        uint4 q[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
+        if (nodeCount) ++*nodeCount;
+        uint32_t hits = node_hits(r, q, tnear, tHit);
+        ng = make_uint2(q[1].x, (hits & 0xff000000u) | (q[0].w >> 24));
+        uint32_t tbits = hits & 0x00ffffffu;
+        uint32_t tbase = q[1].y;
+        while (tbits)
+        {
+            uint32_t tb = 31u - __clz(tbits);
+            tbits &= ~(1u << tb);
+            int ti = (int)(tbase + tb);
+            const float4* tp = reinterpret_cast<const float4*>(sc.tris + ti);
+            float4 a = __ldg(tp), bq = __ldg(tp + 1), c = __ldg(tp + 2);
+            int prim = __float_as_int(a.w);
+            float t, u, v;
+            if (tri_test(r, f3(a.x, a.y, a.z), f3(bq.x, bq.y, bq.z), f3(c.x, c.y, c.z), tnear, tHit, prim, primHit, t,
+                         u, v))
+            {
+                tHit = t;
+                primHit = prim;
+                uHit = u;
+                vHit = v;
+                triHit = ti;
+                if (anyHit) return triHit;
+            }
+        }
+        if (!(ng.y & 0xff000000u))
+        {
+            if (st.sp == 0) break;
+            ng = st.pop();
+        }
+    }
+    return triHit;
+}
+
+// Post-intersection shading and the diffuse bounce
+// (geometry/triangle_mesh.cpp:59-100 + render/diffuse_integrator_single.h:57-63):
+// hit point, eps = max(t, max|p|) * 0x1.fp-18 (core/ray.h:71-76), geometric
+// normal flipped against the ray, frame from makeFrame (math/basis3.h:128-137),
+// cosine-weighted direction (sampling/shape_sampler.h:50-74), and the origin
+// offset by eps along the new direction (core/ray.h:47-52).
+__device__ __forceinline__ void diffuse_bounce(const TriRec* tris, int triIdx, float3& org, float3& dir, float t,
+                                               uint32_t& rng)
+{
+    float3 p = madd(org, t, dir);
+    float m = fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z)));
+    float eps = __fmul_rn(fmaxf(t, m), 0x1.fp-18f);
+    const float4* tp = reinterpret_cast<const float4*>(tris + triIdx);
+    float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    float3 p0 = f3(a.x, a.y, a.z), p1 = f3(b.x, b.y, b.z), p2 = f3(c.x, c.y, c.z);
+    float3 Ng = normalize(cross(sub(p1, p0), sub(p2, p0)));
+    if (dot(Ng, dir) > 0.0f) Ng = f3(-Ng.x, -Ng.y, -Ng.z);
+    // makeFrame
+    float3 U0 = f3(0.0f, Ng.z, -Ng.y);
+    float3 U1 = f3(-Ng.z, 0.0f, Ng.x);
+    float3 U = normalize(dot(U0, U0) > dot(U1, U1) ? U0 : U1);
+    float3 V = normalize(cross(Ng, U));
+    // cosine-weighted hemisphere sample
+    float sx = rng_next(rng);
+    float sy = rng_next(rng);
+    float cosT = __fsqrt_rn(sx);
+    float sinT = __fsqrt_rn(__fsub_rn(1.0f, sx));
+    float sphi, cphi;
+    sincosf(__fmul_rn(2.0f * 3.14159265358979f, sy), &sphi, &cphi);
+    float lx = __fmul_rn(cphi, sinT), ly = __fmul_rn(sphi, sinT);
+    float3 nd = add(add(mul(U, lx), mul(V, ly)), mul(Ng, cosT));
+    dir = nd;
+    org = madd(p, eps, nd);
+}
+
+// Fire-and-forget vector add into the accumulation buffer (sm_90+).
+__device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float c, float d)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
+} // namespace prt_b200

@@ -1,0 +1,113 @@
+// Internal host-side declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/prt_b200.h"
+#include "prt_device.cuh"
+
+namespace prt_b200 {
+
+struct Bvh8Device
+{
+    Bvh8Node* nodes = nullptr;
+    TriRec* tris = nullptr;
+    int nodeCount = 0;
+    int triCount = 0;
+    int levels = 0;
+
+    void release()
+    {
+        if (nodes) cudaFree(nodes);
+        if (tris) cudaFree(tris);
+        nodes = nullptr;
+        tris = nullptr;
+        nodeCount = triCount = levels = 0;
+    }
+};
+
+struct BuildInfo
+{
+    double buildMs = 0;
+    int nodeCount = 0;
+    int levels = 0;
+};
+
+int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
+               std::string& err, BuildInfo* info);
+
+// Arguments of one wave of the wavefront renderer.
+struct WaveArgs
+{
+    SceneDev scene;
+    CameraDev cam;
+    float4* accum;             // width*height sums (r,g,b,weight)
+    PathRec* qin;              // input queue (depth >= 1)
+    PathRec* qout;             // output queue
+    float* thrIn;              // per-path throughput (albedo mode), or nullptr
+    float* thrOut;
+    int* counts;               // counts[d]: paths entering bounce d (d >= 1)
+    int* fetch;                // fetch[d]: work counters of the persistent loop
+    unsigned long long* rays;  // running total of closest-hit queries
+    const int* passBase;       // device pass counter
+    int passOffset;            // first pass of this wave relative to *passBase
+    int passes;                // passes in this wave
+    int tilesX, tilesY;        // 8x8 pixel tiles covering the frame
+    int maxDepth;
+    float thrConst;            // throughput at this depth when albedo is constant
+    float sky;
+};
+
+// Per-request table entry of the batched renderer.
+struct BatchReq
+{
+    SceneDev scene;
+    CameraDev cam;
+    float4* accum;
+    long long pathBegin;   // first global path index of this request
+    int tilesX, tilesY;
+    int spp;
+    int maxDepth;
+};
+
+struct BatchArgs
+{
+    const BatchReq* reqs;
+    int nreq;
+    long long waveBegin;   // global path index range of this wave
+    long long waveEnd;
+    PathRec* qin;
+    PathRec* qout;
+    int* counts;
+    int* fetch;
+    unsigned long long* rays;
+    int maxDepth;          // largest maxDepth of the batch
+    float sky;
+};
+
+struct LaunchCfg
+{
+    int block = 128;
+    int blocksPerSM = 4;
+    int pathsPerWave = 0;   // 0 = automatic
+};
+
+// Kernel launchers (render.cu).  Each returns the number of launches issued.
+int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s);
+int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n, bool anyHit, float* anyOut,
+                     cudaStream_t s);
+int launch_resolve_ldr(const float4* accum, uint32_t* out, int n, cudaStream_t s);
+int launch_advance_pass(int* passBase, int spp, cudaStream_t s);
+int launch_query(const SceneDev& sc, const RayRec* ray, HitRec* hit, float* pNg, cudaStream_t s);
+int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int pass0, int spp, int maxDepth, float sky,
+                  const float* dL, float* dAlbedo, float* dSky, unsigned long long* rays, bool backward,
+                  cudaStream_t s);
+int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s);
+int launch_fill(float4* p, size_t n, cudaStream_t s);
+
+} // namespace prt_b200

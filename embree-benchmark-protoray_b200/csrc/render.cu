@@ -1,0 +1,513 @@
+// Kernels of the wavefront diffuse path tracer.
+//
+// The reference GPU path (render/diffuse_renderer_cuda.cu:159-212) runs, per
+// pass: generateRaysKernel -> { OptiX Prime closest hit -> cudaMemcpy(counter)
+// -> shadeRaysKernel -> cudaMemcpy(count) } per bounce.  Here one persistent
+// kernel per bounce does traversal, shading, queue compaction and
+// accumulation together; primary rays are generated inside the first bounce
+// kernel; queue sizes stay on the device, so a whole render is launched
+// without host synchronisation (and is captured as a CUDA graph by the API).
+#include "prt_internal.h"
+
+namespace prt_b200 {
+
+namespace {
+
+__device__ __forceinline__ void morton8x8(int m, int& x, int& y)
+{
+    // same order as the reference's mortonTableX/Y (image/morton.cpp)
+    x = (m & 1) | ((m >> 1) & 2) | ((m >> 2) & 4);
+    y = ((m >> 1) & 1) | ((m >> 2) & 2) | ((m >> 3) & 4);
+}
+
+__device__ __forceinline__ PathRec load_path(const PathRec* q, int i)
+{
+    const float4* p = reinterpret_cast<const float4*>(q + i);
+    PathRec r;
+    r.w0 = __ldcs(p);
+    r.w1 = __ldcs(p + 1);
+    return r;
+}
+
+__device__ __forceinline__ void store_path(PathRec* q, int i, float3 org, int tag, float3 dir, uint32_t rng)
+{
+    float4* p = reinterpret_cast<float4*>(q + i);
+    __stcs(p, make_float4(org.x, org.y, org.z, __int_as_float(tag)));
+    __stcs(p + 1, make_float4(dir.x, dir.y, dir.z, __uint_as_float(rng)));
+}
+
+// Warp-aggregated append: one atomic per warp, survivors keep lane order.
+__device__ __forceinline__ int warp_append(bool pred, int* counter)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned m = __ballot_sync(0xffffffffu, pred);
+    int base = 0;
+    if (lane == 0 && m) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+// One bounce of the wavefront over the queue of paths entering `depth`.
+// kFirst: the queue is implicit — item i is (pass, 8x8 tile, Morton index)
+// and the primary ray is generated in registers.
+template <bool kFirst, bool kAlbedo>
+__global__ void __launch_bounds__(256) k_bounce(WaveArgs a, int depth)
+{
+    extern __shared__ uint2 s_stack[];
+    TravStack st;
+    st.sh = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    st.overflow = false;
+    const int lane = threadIdx.x & 31;
+    const int W = a.cam.width, H = a.cam.height;
+    const int perPass = a.tilesX * a.tilesY * 64;
+    int total;
+    int pass0 = 0;
+    if (kFirst)
+    {
+        total = a.passes * perPass;
+        pass0 = *a.passBase + a.passOffset;
+    }
+    else
+    {
+        total = *(volatile int*)&a.counts[depth];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(a.rays, kFirst ? (unsigned long long)a.passes * (unsigned long long)W * (unsigned long long)H
+                                 : (unsigned long long)total);
+    const bool final = depth == a.maxDepth;
+    for (;;)
+    {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&a.fetch[depth], 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const int i = base + lane;
+        bool active = i < total;
+        float3 org = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f);
+        int pixel = 0;
+        uint32_t rng = 0;
+        float thr = kAlbedo ? 1.0f : a.thrConst;
+        if (active)
+        {
+            if (kFirst)
+            {
+                int pass = i / perPass;
+                int r = i - pass * perPass;
+                int tile = r >> 6;
+                int mx, my;
+                morton8x8(r & 63, mx, my);
+                int x = (tile % a.tilesX) * 8 + mx;
+                int y = (tile / a.tilesX) * 8 + my;
+                if (x >= W || y >= H)
+                {
+                    active = false;
+                }
+                else
+                {
+                    pixel = x + y * W;
+                    rng = rng_seed(pass0 + pass, pixel);
+                    camera_ray(a.cam, x, y, rng, org, dir);
+                }
+            }
+            else
+            {
+                PathRec pr = load_path(a.qin, i);
+                org = f3(pr.w0.x, pr.w0.y, pr.w0.z);
+                pixel = __float_as_int(pr.w0.w);
+                dir = f3(pr.w1.x, pr.w1.y, pr.w1.z);
+                rng = __float_as_uint(pr.w1.w);
+                if (kAlbedo) thr = __ldcs(a.thrIn + i);
+            }
+        }
+        bool cont = false;
+        float contrib = 0.f;
+        if (active)
+        {
+            TravRay r;
+            trav_setup(r, org, dir);
+            float t, u, v;
+            int prim;
+            int ti = traverse<false>(a.scene, r, 0.0f, FLT_MAX, st, t, prim, u, v);
+            if (ti < 0)
+            {
+                contrib = __fmul_rn(thr, a.sky);
+            }
+            else if (!final)
+            {
+                if (kAlbedo) thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + prim) : 0.8f);
+                diffuse_bounce(a.scene.tris, ti, org, dir, t, rng);
+                cont = true;
+            }
+        }
+        int o = warp_append(cont, &a.counts[depth + 1]);
+        if (cont)
+        {
+            store_path(a.qout, o, org, pixel, dir, rng);
+            if (kAlbedo) __stcs(a.thrOut + o, thr);
+        }
+        else if (active)
+        {
+            red_add_v4(a.accum + pixel, contrib, contrib, contrib, 1.0f);
+        }
+    }
+}
+
+template <bool kAnyHit>
+__global__ void __launch_bounds__(128) k_intersect(SceneDev sc, const RayRec* __restrict__ rays, HitRec* __restrict__ hits,
+                                                   float* __restrict__ anyOut, int n)
+{
+    extern __shared__ uint2 s_stack[];
+    TravStack st;
+    st.sh = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    st.overflow = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const float4* rp = reinterpret_cast<const float4*>(rays + i);
+        float4 a = __ldg(rp), b = __ldg(rp + 1);
+        TravRay r;
+        trav_setup(r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+        float t, u, v;
+        int prim;
+        int ti = traverse<kAnyHit>(sc, r, a.w, b.w, st, t, prim, u, v);
+        if (kAnyHit)
+        {
+            anyOut[i] = ti >= 0 ? t : -1.0f;
+        }
+        else
+        {
+            HitRec h;
+            if (ti >= 0) { h.t = t; h.primId = prim; h.u = u; h.v = v; }
+            else { h.t = -1.0f; h.primId = -1; h.u = 0.f; h.v = 0.f; }
+            reinterpret_cast<float4*>(hits)[i] = make_float4(h.t, __int_as_float(h.primId), h.u, h.v);
+        }
+    }
+}
+
+// Hit point and geometric normal of one query ray (Renderer::queryRay).
+__global__ void k_query(SceneDev sc, const RayRec* ray, HitRec* hit, float* pNg)
+{
+    __shared__ uint2 s_stack[kShared];
+    TravStack st;
+    st.sh = s_stack;
+    st.stride = 1;
+    st.overflow = false;
+    RayRec rr = *ray;
+    TravRay r;
+    trav_setup(r, f3(rr.ox, rr.oy, rr.oz), f3(rr.dx, rr.dy, rr.dz));
+    float t, u, v;
+    int prim;
+    int ti = traverse<false>(sc, r, rr.tnear, rr.tfar, st, t, prim, u, v);
+    if (ti < 0)
+    {
+        *hit = HitRec{-1.0f, -1, 0.f, 0.f};
+        return;
+    }
+    *hit = HitRec{t, prim, u, v};
+    float3 p = madd(r.org, t, r.dir);
+    const TriRec tr = sc.tris[ti];
+    float3 p0 = f3(tr.v0.x, tr.v0.y, tr.v0.z), p1 = f3(tr.v1.x, tr.v1.y, tr.v1.z), p2 = f3(tr.v2.x, tr.v2.y, tr.v2.z);
+    float3 Ng = normalize(cross(sub(p1, p0), sub(p2, p0)));
+    if (dot(Ng, r.dir) > 0.0f) Ng = f3(-Ng.x, -Ng.y, -Ng.z);
+    pNg[0] = p.x; pNg[1] = p.y; pNg[2] = p.z;
+    pNg[3] = Ng.x; pNg[4] = Ng.y; pNg[5] = Ng.z;
+}
+
+// Gamma-2.2 BGRA8 resolve (image/accum_buffer_cuda.cu:22-37; channel order of
+// encodeBgr8, image/pixel.h:42-46).
+__global__ void k_resolve_ldr(const float4* __restrict__ accum, uint32_t* __restrict__ out, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 a = accum[i];
+    float w = a.w > 0.f ? 1.0f / a.w : 0.0f;
+    const float g = 1.0f / 2.2f;
+    int r = min(max((int)(powf(a.x * w, g) * 255.0f), 0), 255);
+    int gg = min(max((int)(powf(a.y * w, g) * 255.0f), 0), 255);
+    int b = min(max((int)(powf(a.z * w, g) * 255.0f), 0), 255);
+    out[i] = (uint32_t)b | ((uint32_t)gg << 8) | ((uint32_t)r << 16);
+}
+
+__global__ void k_advance_pass(int* passBase, int spp) { *passBase += spp; }
+
+constexpr int kReplayMaxDepth = 16;
+
+// Path-replay megakernel: one thread per (pass, pixel) path.  The forward
+// mode accumulates the path's radiance; the backward mode re-traces the same
+// path from its seed and scatters dL/d(radiance) into the albedo of every
+// triangle the path bounced off and into the sky radiance:
+//   radiance = sky * prod_k albedo[prim_k]
+//   d radiance / d albedo[prim_k] = radiance / albedo[prim_k]
+//   d radiance / d sky            = prod_k albedo[prim_k]
+template <bool kBackward>
+__global__ void __launch_bounds__(128) k_replay(SceneDev sc, CameraDev cam, float4* accum, int pass0, int spp,
+                                                int maxDepth, float sky, const float* __restrict__ dL,
+                                                float* dAlbedo, float* dSky, unsigned long long* rays)
+{
+    extern __shared__ uint2 s_stack[];
+    TravStack st;
+    st.sh = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    st.overflow = false;
+    const int W = cam.width, H = cam.height;
+    const long long total = (long long)spp * W * H;
+    float skyGrad = 0.f;
+    unsigned long long myRays = 0;
+    for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < total;
+         gi += (long long)gridDim.x * blockDim.x)
+    {
+        int pass = (int)(gi / ((long long)W * H));
+        int pixel = (int)(gi - (long long)pass * W * H);
+        int x = pixel % W, y = pixel / W;
+        float g = 0.f;
+        if (kBackward)
+        {
+            g = dL[3 * (size_t)pixel] + dL[3 * (size_t)pixel + 1] + dL[3 * (size_t)pixel + 2];
+            if (g == 0.f) continue;
+        }
+        uint32_t rng = rng_seed(pass0 + pass, pixel);
+        float3 org, dir;
+        camera_ray(cam, x, y, rng, org, dir);
+        float thr = 1.0f;
+        int prims[kReplayMaxDepth];
+        int np = 0;
+        bool escaped = false;
+        for (int depth = 0;; ++depth)
+        {
+            TravRay r;
+            trav_setup(r, org, dir);
+            float t, u, v;
+            int prim;
+            int ti = traverse<false>(sc, r, 0.0f, FLT_MAX, st, t, prim, u, v);
+            ++myRays;
+            if (ti < 0) { escaped = true; break; }
+            if (depth == maxDepth) break;
+            thr = __fmul_rn(thr, sc.albedo ? __ldg(sc.albedo + prim) : 0.8f);
+            if (kBackward) prims[np++] = prim;
+            diffuse_bounce(sc.tris, ti, org, dir, t, rng);
+        }
+        float c = escaped ? __fmul_rn(thr, sky) : 0.0f;
+        if (!kBackward)
+        {
+            red_add_v4(accum + pixel, c, c, c, 1.0f);
+        }
+        else if (escaped)
+        {
+            skyGrad += g * thr;
+            float gc = g * c;
+            for (int k = 0; k < np; ++k)
+            {
+                float a = sc.albedo ? __ldg(sc.albedo + prims[k]) : 0.8f;
+                atomicAdd(dAlbedo + prims[k], gc / a);
+            }
+        }
+    }
+    // warp-reduce the counters, one atomic per warp
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        skyGrad += __shfl_down_sync(0xffffffffu, skyGrad, off);
+        myRays += __shfl_down_sync(0xffffffffu, myRays, off);
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        if (kBackward && skyGrad != 0.f) atomicAdd(dSky, skyGrad);
+        if (rays) atomicAdd(rays, myRays);
+    }
+}
+
+// Batched bounce: the paths of many requests share one queue.  Item i of the
+// first bounce is a global path index resolved to (request, pass, tile,
+// Morton index) by a binary search over the requests' path ranges; later
+// bounces carry (request << 24 | pixel) in the path record.
+template <bool kFirst>
+__global__ void __launch_bounds__(256) k_batch_bounce(BatchArgs a, int depth)
+{
+    extern __shared__ uint2 s_dyn[];
+    uint2* s_stack = s_dyn;
+    long long* s_begin = reinterpret_cast<long long*>(s_dyn + kShared * blockDim.x);
+    for (int r = threadIdx.x; r < a.nreq; r += blockDim.x) s_begin[r] = a.reqs[r].pathBegin;
+    __syncthreads();
+    TravStack st;
+    st.sh = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    st.overflow = false;
+    const int lane = threadIdx.x & 31;
+    long long total = kFirst ? (a.waveEnd - a.waveBegin) : (long long)*(volatile int*)&a.counts[depth];
+    if (!kFirst && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.rays, (unsigned long long)total);
+    unsigned long long myRays = 0;
+    for (;;)
+    {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&a.fetch[depth], 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const int i = base + lane;
+        bool active = i < total;
+        float3 org = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f);
+        int pixel = 0, req = 0;
+        uint32_t rng = 0;
+        if (active)
+        {
+            if (kFirst)
+            {
+                long long gi = a.waveBegin + i;
+                int lo = 0, hi = a.nreq - 1;
+                while (lo < hi)
+                {
+                    int mid = (lo + hi + 1) >> 1;
+                    if (s_begin[mid] <= gi) lo = mid;
+                    else hi = mid - 1;
+                }
+                req = lo;
+                const BatchReq& R = a.reqs[req];
+                long long local = gi - R.pathBegin;
+                int perPass = R.tilesX * R.tilesY * 64;
+                int pass = (int)(local / perPass);
+                int rr = (int)(local - (long long)pass * perPass);
+                int tile = rr >> 6;
+                int mx, my;
+                morton8x8(rr & 63, mx, my);
+                int x = (tile % R.tilesX) * 8 + mx;
+                int y = (tile / R.tilesX) * 8 + my;
+                if (x >= R.cam.width || y >= R.cam.height)
+                {
+                    active = false;
+                }
+                else
+                {
+                    pixel = x + y * R.cam.width;
+                    rng = rng_seed(pass, pixel);
+                    camera_ray(R.cam, x, y, rng, org, dir);
+                    ++myRays;
+                }
+            }
+            else
+            {
+                PathRec pr = load_path(a.qin, i);
+                org = f3(pr.w0.x, pr.w0.y, pr.w0.z);
+                int tag = __float_as_int(pr.w0.w);
+                req = (int)((uint32_t)tag >> 24);
+                pixel = tag & 0xffffff;
+                dir = f3(pr.w1.x, pr.w1.y, pr.w1.z);
+                rng = __float_as_uint(pr.w1.w);
+            }
+        }
+        bool cont = false;
+        float contrib = 0.f;
+        float4* accum = nullptr;
+        if (active)
+        {
+            const BatchReq& R = a.reqs[req];
+            accum = R.accum;
+            TravRay r;
+            trav_setup(r, org, dir);
+            float t, u, v;
+            int prim;
+            int ti = traverse<false>(R.scene, r, 0.0f, FLT_MAX, st, t, prim, u, v);
+            if (ti < 0)
+            {
+                float thr = 1.0f;
+                for (int d = 0; d < depth; ++d) thr = __fmul_rn(thr, 0.8f);
+                contrib = __fmul_rn(thr, a.sky);
+            }
+            else if (depth < R.maxDepth)
+            {
+                diffuse_bounce(R.scene.tris, ti, org, dir, t, rng);
+                cont = true;
+            }
+        }
+        int o = warp_append(cont, &a.counts[depth + 1]);
+        if (cont) store_path(a.qout, o, org, (req << 24) | pixel, dir, rng);
+        else if (active) red_add_v4(accum + pixel, contrib, contrib, contrib, 1.0f);
+    }
+    if (kFirst)
+    {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) myRays += __shfl_down_sync(0xffffffffu, myRays, off);
+        if (lane == 0 && myRays) atomicAdd(a.rays, myRays);
+    }
+}
+
+inline int grid_for(int numSMs, const LaunchCfg& cfg) { return numSMs * cfg.blocksPerSM; }
+
+} // namespace
+
+int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
+{
+    size_t shmem = sizeof(uint2) * kShared * cfg.block;
+    int grid = grid_for(numSMs, cfg);
+    bool albedo = a.thrIn != nullptr || a.thrOut != nullptr;
+    if (depth == 0)
+    {
+        if (albedo) k_bounce<true, true><<<grid, cfg.block, shmem, s>>>(a, depth);
+        else k_bounce<true, false><<<grid, cfg.block, shmem, s>>>(a, depth);
+    }
+    else
+    {
+        if (albedo) k_bounce<false, true><<<grid, cfg.block, shmem, s>>>(a, depth);
+        else k_bounce<false, false><<<grid, cfg.block, shmem, s>>>(a, depth);
+    }
+    return 1;
+}
+
+int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
+{
+    size_t shmem = sizeof(uint2) * kShared * cfg.block + sizeof(long long) * a.nreq;
+    int grid = grid_for(numSMs, cfg);
+    if (depth == 0) k_batch_bounce<true><<<grid, cfg.block, shmem, s>>>(a, depth);
+    else k_batch_bounce<false><<<grid, cfg.block, shmem, s>>>(a, depth);
+    return 1;
+}
+
+int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n, bool anyHit, float* anyOut,
+                     cudaStream_t s)
+{
+    if (n <= 0) return 0;
+    int block = 128;
+    int grid = (n + block - 1) / block;
+    if (grid > 148 * 16) grid = 148 * 16;
+    size_t shmem = sizeof(uint2) * kShared * block;
+    if (anyHit) k_intersect<true><<<grid, block, shmem, s>>>(sc, rays, hits, anyOut, n);
+    else k_intersect<false><<<grid, block, shmem, s>>>(sc, rays, hits, anyOut, n);
+    return 1;
+}
+
+int launch_query(const SceneDev& sc, const RayRec* ray, HitRec* hit, float* pNg, cudaStream_t s)
+{
+    k_query<<<1, 1, 0, s>>>(sc, ray, hit, pNg);
+    return 1;
+}
+
+int launch_resolve_ldr(const float4* accum, uint32_t* out, int n, cudaStream_t s)
+{
+    if (n <= 0) return 0;
+    k_resolve_ldr<<<(n + 255) / 256, 256, 0, s>>>(accum, out, n);
+    return 1;
+}
+
+int launch_advance_pass(int* passBase, int spp, cudaStream_t s)
+{
+    k_advance_pass<<<1, 1, 0, s>>>(passBase, spp);
+    return 1;
+}
+
+int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int pass0, int spp, int maxDepth, float sky,
+                  const float* dL, float* dAlbedo, float* dSky, unsigned long long* rays, bool backward,
+                  cudaStream_t s)
+{
+    long long total = (long long)spp * cam.width * cam.height;
+    if (total <= 0) return 0;
+    int block = 128;
+    long long g = (total + block - 1) / block;
+    int grid = (int)(g < 148LL * 32 ? g : 148LL * 32);
+    size_t shmem = sizeof(uint2) * kShared * block;
+    if (backward) k_replay<true><<<grid, block, shmem, s>>>(sc, cam, accum, pass0, spp, maxDepth, sky, dL, dAlbedo, dSky, rays);
+    else k_replay<false><<<grid, block, shmem, s>>>(sc, cam, accum, pass0, spp, maxDepth, sky, dL, dAlbedo, dSky, rays);
+    return 1;
+}
+
+int replay_max_depth() { return kReplayMaxDepth; }
+
+} // namespace prt_b200

@@ -1,0 +1,206 @@
+/*
+ * prt_b200 — C ABI of the B200 wavefront diffuse path tracer.
+ *
+ * This is the drop-in boundary for ProtoRay's GPU rendering path.  Each
+ * entry point names the reference interface it replaces (paths relative to
+ * the ProtoRay tree).  The signatures use only plain C types, pointers and
+ * sizes; CUDA streams are passed as `void*` (a cudaStream_t, or NULL for the
+ * context's own stream).
+ *
+ * Memory: bulk buffers given to prt_read_accum, prt_set_albedo,
+ * prt_render_backward and prt_request.accum may be host or device pointers
+ * (resolved with cudaPointerGetAttributes); device pointers are used in
+ * place.  prt_intersect / prt_occluded take device pointers and borrow them
+ * for the call only.
+ *
+ * Errors: every entry point returns a prt_status; prt_last_error() returns
+ * the message of the last failure on that context.  The reference reports the
+ * same conditions with C++ exceptions (render/device_cuda.cpp:63,92,
+ * render/diffuse_renderer_cuda.cu:161-162, sys/memory_cuda.h:115-116).
+ *
+ * Threading: a context belongs to one host thread at a time; it owns one
+ * CUDA stream on its device.
+ */
+#ifndef PRT_B200_H
+#define PRT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PRT_OK = 0,
+    PRT_EINVAL = 1,     /* invalid argument (std::invalid_argument / std::logic_error in the reference) */
+    PRT_ENOMEM = 2,     /* device allocation failed (std::runtime_error, sys/memory_cuda.h:115-116) */
+    PRT_ECUDA = 3,      /* CUDA runtime or launch error */
+    PRT_ETIMEOUT = 4,   /* a bounded device wait expired */
+    PRT_EINTERNAL = 5,  /* internal consistency check failed */
+    PRT_EIO = 6,        /* file missing, truncated or with a wrong blob id (sys/blob.h:26-38) */
+    PRT_ESTATE = 7      /* call out of order (e.g. render before build) */
+} prt_status;
+
+typedef struct prt_ctx prt_ctx;
+
+/* View record of a .view file (main/render/view.h:25-33). */
+typedef struct {
+    float pos[3];
+    float angleX, angleY, fovY;
+    float radius;   /* lens radius; 0 = pinhole */
+    float focus;    /* focal distance */
+} prt_view;
+
+/* Camera fields of ThinLensCameraCuda (camera/thin_lens_camera_cuda.h:23-30,
+ * camera/pinhole_camera_cuda.h). lensRadius == 0 selects the pinhole camera. */
+typedef struct {
+    float origin[3];
+    float basisU[3], basisV[3];
+    float imageO[3], imageDx[3], imageDy[3];
+    float lensRadius, focalDistance;
+} prt_camera;
+
+/* RayCuda (core/ray_cuda.cuh:47-80): 32 bytes. */
+typedef struct {
+    float org[3];
+    float tnear;
+    float dir[3];
+    float tfar;
+} prt_ray;
+
+/* HitCuda (core/ray_cuda.cuh:23-35): 16 bytes; a miss has t < 0. */
+typedef struct {
+    float t;
+    int primId;
+    float u, v;
+} prt_hit;
+
+/* Stats of the acceleration build: the reference reports buildMs/buildMprim
+ * (accel/optix/optix_intersector_stream_cuda.cpp:62-70). */
+typedef struct {
+    double buildMs;
+    double buildMprim;
+    int nodeCount;   /* 8-wide nodes */
+    int levels;      /* tree depth in 8-wide levels */
+} prt_build_stats;
+
+/* Stats of one render call: ray = closest-hit queries, counted as the
+ * reference counts them (render/diffuse_renderer_cuda.cu:185-186);
+ * mray = rays / 1e6 / seconds of device time (render/device_cuda.cpp:99-105). */
+typedef struct {
+    long long rays;
+    double ms;
+    double mray;
+    int passes;
+} prt_render_stats;
+
+/* One request of a batched render (no reference counterpart; see prt_render_batch). */
+typedef struct {
+    prt_ctx* scene;     /* context whose mesh and acceleration structure are rendered */
+    prt_camera camera;
+    int width, height;
+    int spp;            /* passes, starting at pass 0 */
+    int maxDepth;
+    float* accum;       /* width*height*4 floats (sum r, g, b, weight), host or device, overwritten */
+} prt_request;
+
+/* Autotuned launch configuration. */
+typedef struct {
+    int blockSize;        /* threads per block of the bounce kernel */
+    int blocksPerSM;      /* resident blocks per SM of the persistent grid */
+    int pathsPerWave;     /* queue capacity (paths in flight per wave) */
+    double mray;          /* throughput measured for the winner */
+} prt_tune;
+
+/* --- context (DeviceCuda construction, render/device_cuda.cpp:31-49) --- */
+int prt_create(int device, prt_ctx** out);
+int prt_destroy(prt_ctx* ctx);
+const char* prt_last_error(const prt_ctx* ctx);
+/* Device name, as Device::getInfo (render/device.h:34). */
+int prt_get_info(prt_ctx* ctx, char* buf, int len);
+
+/* --- scene (DeviceCuda::initScene, render/device_cuda.cpp:121-168) --- */
+/* Copies a triangle mesh: indices int32[triCount][3], positions float[vertCount][3]. */
+int prt_load_mesh(prt_ctx* ctx, const int* indices, int triCount, const float* positions, int vertCount);
+/* Loads a .mesh blob (geometry/triangle_mesh.cpp:305-320, sys/blob.h:26-38);
+ * bounds (nullable) receive the stored scene box. */
+int prt_load_mesh_file(prt_ctx* ctx, const char* path, float boundsLo[3], float boundsHi[3]);
+/* Scene bounds (Device::getSceneBounds, render/device.h:38). */
+int prt_get_scene_bounds(prt_ctx* ctx, float lo[3], float hi[3]);
+/* Per-triangle diffuse albedo (NULL restores the constant 0.8 of
+ * render/diffuse_integrator_single.h:43) and sky radiance (1 in the reference). */
+int prt_set_albedo(prt_ctx* ctx, const float* albedo, int triCount);
+int prt_set_sky(prt_ctx* ctx, float sky);
+
+/* --- acceleration structure (OptixIntersectorStreamCuda ctor, accel/optix/optix_intersector_stream_cuda.cpp:23-75) --- */
+int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats);
+
+/* --- camera (DeviceCuda::initCamera, render/device_cuda.cpp:175-200) --- */
+/* Builds the camera of a view for an image of width x height, as the
+ * reference viewer does (main/render/render_window.cpp:307-325 with
+ * camera/pinhole_camera.h:34-47). */
+int prt_camera_from_view(const prt_view* view, int width, int height, prt_camera* cam);
+int prt_set_camera(prt_ctx* ctx, const prt_camera* cam);
+
+/* --- frame (DeviceCuda::initFrame / clearFrame / blitFrame, render/device_cuda.cpp:202-230) --- */
+int prt_init_frame(prt_ctx* ctx, int width, int height);
+int prt_clear(prt_ctx* ctx);
+/* Accumulation buffer, width*height*4 floats (sum r, g, b, weight) in raster
+ * order (AccumBufferCuda, image/accum_buffer_cuda.h:23-29). */
+int prt_read_accum(prt_ctx* ctx, float* rgbw);
+/* Gamma-2.2 BGRA8 resolve (accumBufferUpdateKernel, image/accum_buffer_cuda.cu:22-37). */
+int prt_read_ldr(prt_ctx* ctx, uint32_t* bgra);
+
+/* --- rendering (DiffuseRendererCuda::render, render/diffuse_renderer_cuda.cu:159-212) --- */
+/* Renders `spp` passes of the diffuse path tracer (one path per pixel per
+ * pass, up to maxDepth bounces).  accumulate = 0 clears the frame first (the
+ * "Fast" renderers' overwrite, render/renderer_factory_single.cpp:58-59).
+ * Passes continue from the previous call until prt_clear / prt_set_pass. */
+int prt_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, prt_render_stats* stats);
+/* Pass counter of the next render (RendererSingle::pass, render/renderer_single.h:97-98). */
+int prt_set_pass(prt_ctx* ctx, int pass);
+int prt_get_pass(prt_ctx* ctx, int* pass);
+
+/* --- queries (Renderer::queryRay, render/renderer_single.h:137-163;
+ *     DeviceCuda::queryRay returns nothing in the reference, render/device_cuda.cpp:111-119) --- */
+/* p and Ng (nullable) receive the hit point and the geometric normal facing the ray. */
+int prt_query_ray(prt_ctx* ctx, const prt_ray* ray, prt_hit* hit, float p[3], float Ng[3]);
+
+/* --- intersector seam (IntersectorStreamCuda, core/intersector_stream_cuda.h:32-33) --- */
+/* Closest hit for n rays (device pointers); misses get t = -1. */
+int prt_intersect(prt_ctx* ctx, const prt_ray* rays, prt_hit* hits, int n, void* stream);
+/* Any hit for n rays (device pointers); out[i] = t of some hit, or -1 (AnyHitCuda). */
+int prt_occluded(prt_ctx* ctx, const prt_ray* rays, float* out, int n, void* stream);
+
+/* --- differentiation (no reference counterpart) --- */
+/* Path-replay adjoint of the last prt_render configuration: given
+ * dL/dsum (width*height*3 floats, gradient of the loss with respect to the
+ * accumulated r,g,b sums of passes [pass0, pass0+spp)), writes
+ * d_albedo (triCount floats) and d_sky (1 float).  Paths are recomputed from
+ * their (pixel, pass) seeds; nothing from the forward pass is stored. */
+int prt_render_backward(prt_ctx* ctx, int pass0, int spp, int maxDepth, const float* dL_dsum, float* d_albedo,
+                        float* d_sky);
+/* Forward render of passes [pass0, pass0+spp) with the same path code as
+ * prt_render_backward (for gradient checks); adds into the frame. */
+int prt_render_replay(prt_ctx* ctx, int pass0, int spp, int maxDepth, prt_render_stats* stats);
+
+/* --- batching (no reference counterpart) --- */
+/* Renders n requests of uneven resolution, spp and scene in shared waves of
+ * one persistent kernel per bounce (CUDA-graph captured), on ctx's device. */
+int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_stats* stats);
+
+/* --- launch configuration --- */
+/* Times candidate bounce-kernel configurations on the current scene/frame
+ * and keeps the fastest for later renders. */
+int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best);
+int prt_set_tune(prt_ctx* ctx, const prt_tune* tune);
+int prt_get_tune(prt_ctx* ctx, prt_tune* tune);
+
+/* Kernel launches issued by this context since creation (for accounting). */
+long long prt_launch_count(prt_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,169 @@
+"""Parity of the CUDA path with the FP64 oracle (all through the C ABI).
+
+Tolerances (from the hot-path contract):
+* primary-hit primitive ids bit-exact except on grazing ties / edges, which
+  the FP64 oracle flags; unflagged mismatches must stay below 1e-5 of rays;
+* images at the same seed and spp within a mean per-pixel relative error of
+  1e-3 (|gpu - oracle| / max(oracle, 1e-2), red channel sums).
+"""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx_small(small):
+    import prt
+    mesh, view = small
+    c = prt.Context(0)
+    c.load_mesh(mesh.indices, mesh.positions)
+    c.build()
+    return c
+
+
+def _intersect(ctx, rays_np):
+    n = len(rays_np)
+    rays = torch.from_numpy(np.ascontiguousarray(rays_np, np.float32)).cuda()
+    hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    ctx.intersect(rays, hits, n)
+    torch.cuda.synchronize()
+    return hits.cpu().numpy()
+
+
+def test_primary_hit_ids_match_oracle(ctx_small, small, small_oracle, oracle_mod):
+    mesh, view = small
+    O = oracle_mod.Oracle()
+    W, H = 256, 256
+    for p in (0, 7):
+        cam = O.camera(view, W, H)
+        rays = O.primary_rays(cam, W, H, p)
+        ref, flags = small_oracle.intersect(rays, flags=True)
+        got = _intersect(ctx_small, rays)
+        rp = ref[:, 1].view(np.int32)
+        gp = got[:, 1].view(np.int32)
+        mism = rp != gp
+        unflagged = mism & (flags == 0)
+        assert unflagged.sum() <= 1e-5 * len(rays), (mism.sum(), unflagged.sum())
+        hit = (rp >= 0) & ~mism
+        np.testing.assert_allclose(got[hit, 0], ref[hit, 0], rtol=2e-5)
+        np.testing.assert_allclose(got[hit, 2:], ref[hit, 2:], atol=2e-4)
+        assert np.all(got[rp < 0, 0] < 0) or mism.any()
+
+
+def test_incoherent_rays_match_oracle(ctx_small, small_oracle):
+    rng = np.random.default_rng(5)
+    n = 20000
+    org = rng.uniform(-12, 12, size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, :3] = org
+    rays[:, 4:7] = d
+    rays[:, 7] = 3.0e38
+    rays[::3, 7] = 5.0          # short segments exercise tfar
+    rays[1::7, 3] = 0.5         # and tnear
+    ref, flags = small_oracle.intersect(rays, flags=True)
+    got = _intersect(ctx_small, rays)
+    rp = ref[:, 1].view(np.int32)
+    gp = got[:, 1].view(np.int32)
+    mism = (rp != gp) & (flags == 0)
+    assert mism.sum() <= max(1, 1e-4 * n), mism.sum()
+    ok = (rp >= 0) & (rp == gp)
+    np.testing.assert_allclose(got[ok, 0], ref[ok, 0], rtol=1e-4, atol=1e-5)
+
+
+def test_occluded_matches_closest_hit(ctx_small, small_oracle):
+    rng = np.random.default_rng(6)
+    n = 8192
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, :3] = rng.uniform(-12, 12, size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 7] = rng.uniform(0.5, 30.0, size=n)
+    ref = small_oracle.occluded(rays)
+    r = torch.from_numpy(rays).cuda()
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    ctx_small.occluded(r, out, n)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    closest = small_oracle.intersect(rays)
+    near_end = np.abs(closest[:, 0] - rays[:, 7]) < 1e-4 * rays[:, 7]
+    agree = ((got >= 0) == (ref >= 0)) | near_end
+    assert agree.mean() > 1 - 1e-4
+    hit = got >= 0
+    assert np.all(got[hit] <= rays[hit, 7] * (1 + 1e-5))
+
+
+def _rel_err(a, b):
+    return float(np.mean(np.abs(a - b) / np.maximum(np.abs(b), 1e-2)))
+
+
+@pytest.mark.parametrize("lens", [0.0, 0.3])
+def test_image_parity_small(ctx_small, small, small_oracle, oracle_mod, lens):
+    """256x256, 16 spp, maxDepth 5 on the ~82K-triangle scene."""
+    import scenes
+    import prt
+    mesh, view = small
+    W, H, spp, depth = 256, 256, 16, 5
+    v = scenes.View(view.pos, view.angleX, view.angleY, view.fovY, lens, 38.0 if lens else view.focus)
+    ctx_small.init_frame(W, H)
+    ctx_small.set_view(v, W, H)
+    st = ctx_small.render(spp, depth)
+    img = ctx_small.read_accum()
+    cam = oracle_mod.Oracle().camera(v, W, H)
+    ref, rays = small_oracle.render(cam, W, H, 0, spp, depth)
+    assert np.all(img[..., 3] == spp)
+    err = _rel_err(img[..., 0], ref[..., 0])
+    assert err < 1e-3, err
+    assert abs(st["ray"] - rays) <= 1e-3 * rays
+    assert ctx_small.get_pass() == spp
+
+
+def test_progressive_passes_equal_single_call(ctx_small, small):
+    mesh, view = small
+    W, H = 64, 48
+    ctx_small.init_frame(W, H)
+    ctx_small.set_view(view, W, H)
+    ctx_small.render(6, 4)
+    a = ctx_small.read_accum().copy()
+    ctx_small.clear()
+    for _ in range(3):
+        ctx_small.render(2, 4)
+    b = ctx_small.read_accum()
+    np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-6)
+
+
+def test_fast_mode_overwrites(ctx_small, small):
+    mesh, view = small
+    ctx_small.init_frame(32, 32)
+    ctx_small.set_view(view, 32, 32)
+    ctx_small.render(3, 3, accumulate=False)
+    ctx_small.render(1, 3, accumulate=False)
+    img = ctx_small.read_accum()
+    assert np.all(img[..., 3] == 1)
+
+
+def test_ldr_resolve(ctx_small, small):
+    mesh, view = small
+    W, H = 40, 24
+    ctx_small.init_frame(W, H)
+    ctx_small.set_view(view, W, H)
+    ctx_small.render(4, 3)
+    acc = ctx_small.read_accum()
+    ldr = ctx_small.read_ldr()
+    c = acc[..., :3] / acc[..., 3:4]
+    exp = np.clip((np.power(c, 1 / 2.2) * 255.0).astype(np.int64), 0, 255)
+    bgr = (exp[..., 2] | (exp[..., 1] << 8) | (exp[..., 0] << 16)).astype(np.uint32)
+    assert np.mean(np.abs(ldr.astype(np.int64) - bgr.astype(np.int64)) <= 1) == 1.0
+
+
+def test_query_ray(ctx_small, golden):
+    for r, prim, dist, ng in zip(golden["query_in"], golden["query_prim"], golden["query_dist"], golden["query_Ng"]):
+        q = ctx_small.query_ray(r[:3], r[4:7])
+        assert q is not None and q["primId"] == prim
+        assert abs(q["dist"] - dist) <= 1e-5 * dist
+        np.testing.assert_allclose(q["Ng"], ng, atol=1e-5)

@@ -331,12 +331,17 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and fwd+bwd measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--width", type=int, default=W, help="smaller frames are for profiling captures only")
+    ap.add_argument("--height", type=int, default=H)
+    ap.add_argument("--spp", type=int, default=SPP)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
     if args.impl == "reference":
         return run_reference(args)
+    global W, H, SPP
+    W, H, SPP = args.width, args.height, args.spp
 
     rank, world, local = dist_env()
     import torch

@@ -743,6 +743,76 @@ int prt_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, prt_render_s
     return finish_stats(ctx, stats, spp);
 }
 
+int prt_render_profile(prt_ctx* ctx, int spp, int maxDepth, double* msPerDepth, long long* raysPerDepth)
+{
+    int st = check_ready(ctx, true);
+    if (st != PRT_OK) return st;
+    if (spp <= 0 || maxDepth < 0 || maxDepth > kMaxDepthCap || !msPerDepth || !raysPerDepth)
+        return fail(ctx, PRT_EINVAL, "invalid spp, maxDepth or output arrays");
+    CK(cudaSetDevice(ctx->device));
+    const int W = ctx->W, H = ctx->H;
+    const int tilesX = (W + 7) / 8, tilesY = (H + 7) / 8;
+    const long long perPass = (long long)tilesX * tilesY * 64;
+    const int ppw = passes_per_wave(ctx, spp);
+    const bool albedo = ctx->dAlbedo != nullptr;
+    st = ensure_queues(ctx, (long long)ppw * perPass, albedo);
+    if (st != PRT_OK) return st;
+    for (int d = 0; d <= maxDepth; ++d)
+    {
+        msPerDepth[d] = 0;
+        raysPerDepth[d] = 0;
+    }
+    std::vector<cudaEvent_t> ev((size_t)maxDepth + 2);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    WaveArgs a;
+    a.scene = scene_dev(ctx);
+    a.cam = camera_dev(ctx->cam, W, H);
+    a.accum = ctx->dAccum;
+    a.counts = ctx->dCounts;
+    a.fetch = ctx->dFetch;
+    a.rays = ctx->dRays;
+    a.passBase = ctx->dPass;
+    a.tilesX = tilesX;
+    a.tilesY = tilesY;
+    a.maxDepth = maxDepth;
+    a.sky = ctx->sky;
+    CK(cudaMemsetAsync(ctx->dAccum, 0, sizeof(float4) * (size_t)W * H, ctx->stream));
+    for (int p0 = 0; p0 < spp; p0 += ppw)
+    {
+        a.passOffset = p0;
+        a.passes = std::min(ppw, spp - p0);
+        CK(cudaMemsetAsync(ctx->dCounts, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+        CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+        CK(cudaEventRecord(ev[0], ctx->stream));
+        for (int d = 0; d <= maxDepth; ++d)
+        {
+            a.qin = d == 0 ? nullptr : ctx->q[(d - 1) & 1];
+            a.qout = ctx->q[d & 1];
+            a.thrIn = albedo && d > 0 ? ctx->thr[(d - 1) & 1] : nullptr;
+            a.thrOut = albedo ? ctx->thr[d & 1] : nullptr;
+            a.thrConst = const_throughput(d);
+            ctx->launches += launch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
+            CK(cudaEventRecord(ev[(size_t)d + 1], ctx->stream));
+        }
+        CK(cudaGetLastError());
+        std::vector<int> counts((size_t)maxDepth + 2);
+        CK(cudaMemcpyAsync(counts.data(), ctx->dCounts, sizeof(int) * counts.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int d = 0; d <= maxDepth; ++d)
+        {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ev[(size_t)d], ev[(size_t)d + 1]));
+            msPerDepth[d] += ms;
+            raysPerDepth[d] += d == 0 ? (long long)a.passes * W * H : counts[(size_t)d];
+        }
+    }
+    launch_advance_pass(ctx->dPass, spp, ctx->stream);
+    ctx->launches++;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (auto& e : ev) cudaEventDestroy(e);
+    return PRT_OK;
+}
+
 int prt_query_ray(prt_ctx* ctx, const prt_ray* ray, prt_hit* hit, float p[3], float Ng[3])
 {
     int st = check_ready(ctx, false);
@@ -977,7 +1047,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
 int prt_set_tune(prt_ctx* ctx, const prt_tune* t)
 {
     if (!ctx || !t) return PRT_EINVAL;
-    if (t->blockSize < 32 || t->blockSize > 256 || (t->blockSize & 31) || t->blocksPerSM < 1 || t->blocksPerSM > 64 ||
+    if (t->blockSize < 32 || t->blockSize > 256 || (t->blockSize & 31) || t->blocksPerSM < 0 || t->blocksPerSM > 64 ||
         t->pathsPerWave < 0)
         return fail(ctx, PRT_EINVAL, "invalid launch configuration");
     ctx->cfg.block = t->blockSize;
@@ -1008,12 +1078,11 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
     LaunchCfg bestCfg = saved;
     double bestMray = -1;
     const int blocks[] = {64, 128, 256};
-    const int perSM[] = {2, 4, 8, 16};
+    const int perSM[] = {0, 2, 4};
     const long long waves[] = {1, 2, 4};
     for (int b : blocks)
         for (int s : perSM)
         {
-            if (b * s > 2048) continue;   // more threads than an SM can hold
             for (long long wv : waves)
             {
                 long long ppw = std::max<long long>(perPass * wv, 1 << 16);

@@ -93,7 +93,7 @@ struct BatchArgs
 struct LaunchCfg
 {
     int block = 128;
-    int blocksPerSM = 4;
+    int blocksPerSM = 0;    // 0 = as many as stay resident
     int pathsPerWave = 0;   // 0 = automatic
 };
 

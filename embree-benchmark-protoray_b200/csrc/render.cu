@@ -7,6 +7,8 @@
 // accumulation together; primary rays are generated inside the first bounce
 // kernel; queue sizes stay on the device, so a whole render is launched
 // without host synchronisation (and is captured as a CUDA graph by the API).
+#include <algorithm>
+
 #include "prt_internal.h"
 
 namespace prt_b200 {
@@ -430,24 +432,37 @@ __global__ void __launch_bounds__(256) k_batch_bounce(BatchArgs a, int depth)
     }
 }
 
-inline int grid_for(int numSMs, const LaunchCfg& cfg) { return numSMs * cfg.blocksPerSM; }
+// Persistent grid: cfg.blocksPerSM blocks per SM, capped by (and, when 0,
+// equal to) the number of blocks the kernel can keep resident per SM.
+template <class Kernel>
+int grid_for(Kernel kernel, int block, size_t shmem, int numSMs, const LaunchCfg& cfg)
+{
+    int resident = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, block, shmem) != cudaSuccess || resident < 1)
+        resident = 1;
+    int perSM = cfg.blocksPerSM > 0 ? std::min(cfg.blocksPerSM, resident) : resident;
+    return numSMs * perSM;
+}
 
 } // namespace
 
 int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
 {
     size_t shmem = sizeof(uint2) * kShared * cfg.block;
-    int grid = grid_for(numSMs, cfg);
     bool albedo = a.thrIn != nullptr || a.thrOut != nullptr;
+    auto go = [&](auto kernel) {
+        int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);
+        kernel<<<grid, cfg.block, shmem, s>>>(a, depth);
+    };
     if (depth == 0)
     {
-        if (albedo) k_bounce<true, true><<<grid, cfg.block, shmem, s>>>(a, depth);
-        else k_bounce<true, false><<<grid, cfg.block, shmem, s>>>(a, depth);
+        if (albedo) go(k_bounce<true, true>);
+        else go(k_bounce<true, false>);
     }
     else
     {
-        if (albedo) k_bounce<false, true><<<grid, cfg.block, shmem, s>>>(a, depth);
-        else k_bounce<false, false><<<grid, cfg.block, shmem, s>>>(a, depth);
+        if (albedo) go(k_bounce<false, true>);
+        else go(k_bounce<false, false>);
     }
     return 1;
 }
@@ -455,9 +470,12 @@ int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs
 int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
 {
     size_t shmem = sizeof(uint2) * kShared * cfg.block + sizeof(long long) * a.nreq;
-    int grid = grid_for(numSMs, cfg);
-    if (depth == 0) k_batch_bounce<true><<<grid, cfg.block, shmem, s>>>(a, depth);
-    else k_batch_bounce<false><<<grid, cfg.block, shmem, s>>>(a, depth);
+    auto go = [&](auto kernel) {
+        int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);
+        kernel<<<grid, cfg.block, shmem, s>>>(a, depth);
+    };
+    if (depth == 0) go(k_batch_bounce<true>);
+    else go(k_batch_bounce<false>);
     return 1;
 }
 

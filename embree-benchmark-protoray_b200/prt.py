@@ -29,7 +29,7 @@ EXPORTS = [
     "prt_load_mesh", "prt_load_mesh_file", "prt_get_scene_bounds", "prt_set_albedo", "prt_set_sky",
     "prt_build_accel", "prt_camera_from_view", "prt_set_camera",
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
-    "prt_render", "prt_set_pass", "prt_get_pass", "prt_query_ray",
+    "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
     "prt_render_batch", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_launch_count",
 ]
@@ -107,6 +107,7 @@ def lib() -> C.CDLL:
         "prt_read_accum": (ip, [vp, vp]),
         "prt_read_ldr": (ip, [vp, vp]),
         "prt_render": (ip, [vp, ip, ip, ip, C.POINTER(RenderStats)]),
+        "prt_render_profile": (ip, [vp, ip, ip, vp, vp]),
         "prt_set_pass": (ip, [vp, ip]),
         "prt_get_pass": (ip, [vp, C.POINTER(C.c_int)]),
         "prt_query_ray": (ip, [vp, C.POINTER(Ray), C.POINTER(Hit), vp, vp]),
@@ -228,6 +229,13 @@ class Context:
         s = RenderStats()
         self._check(self.L.prt_render(self.h, spp, max_depth, int(accumulate), C.byref(s)), "prt_render")
         return {"ray": s.rays, "ms": s.ms, "mray": s.mray, "passes": s.passes}
+
+    def render_profile(self, spp: int, max_depth: int):
+        ms = np.zeros(max_depth + 1, np.float64)
+        rays = np.zeros(max_depth + 1, np.int64)
+        self._check(self.L.prt_render_profile(self.h, spp, max_depth, ms.ctypes.data, rays.ctypes.data),
+                    "prt_render_profile")
+        return ms, rays
 
     def render_replay(self, pass0: int, spp: int, max_depth: int) -> Dict[str, float]:
         s = RenderStats()

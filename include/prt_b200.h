@@ -157,6 +157,11 @@ int prt_read_ldr(prt_ctx* ctx, uint32_t* bgra);
  * "Fast" renderers' overwrite, render/renderer_factory_single.cpp:58-59).
  * Passes continue from the previous call until prt_clear / prt_set_pass. */
 int prt_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, prt_render_stats* stats);
+/* Same work as prt_render without graph capture, with CUDA events around
+ * every bounce launch: msPerDepth[d] / raysPerDepth[d] (maxDepth + 1 entries)
+ * receive the device time and closest-hit queries of bounce d, summed over
+ * waves.  The frame is cleared first. */
+int prt_render_profile(prt_ctx* ctx, int spp, int maxDepth, double* msPerDepth, long long* raysPerDepth);
 /* Pass counter of the next render (RendererSingle::pass, render/renderer_single.h:97-98). */
 int prt_set_pass(prt_ctx* ctx, int pass);
 int prt_get_pass(prt_ctx* ctx, int* pass);

@@ -50,7 +50,7 @@ def test_primary_hit_ids_match_oracle(ctx_small, small, small_oracle, oracle_mod
         assert unflagged.sum() <= 1e-5 * len(rays), (mism.sum(), unflagged.sum())
         hit = (rp >= 0) & ~mism
         np.testing.assert_allclose(got[hit, 0], ref[hit, 0], rtol=2e-5)
-        np.testing.assert_allclose(got[hit, 2:], ref[hit, 2:], atol=2e-4)
+        np.testing.assert_allclose(got[hit, 2:], ref[hit, 2:], atol=2e-3)
         assert np.all(got[rp < 0, 0] < 0) or mism.any()
 
 

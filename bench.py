@@ -323,6 +323,7 @@ def run_fwd_bwd(prt, torch, device):
 
 
 def main():
+    global W, H, SPP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -340,7 +341,6 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args)
-    global W, H, SPP
     W, H, SPP = args.width, args.height, args.spp
 
     rank, world, local = dist_env()

@@ -358,64 +358,100 @@ struct TravStack
 
 // Closest hit (anyHit = false) or any hit (anyHit = true) over (tnear, tfar].
 // Returns the leaf-order triangle index of the hit (or -1), with t/u/v/prim.
-template <bool anyHit>
-__device__ __forceinline__ int traverse(const SceneDev& sc, const TravRay& r, float tnear, float tfar, TravStack& st,
-                                        float& tHit, int& primHit, float& uHit, float& vHit, int* nodeCount = nullptr)
+// Resumable traversal state of one ray.  A step visits one 8-wide node and
+// tests the triangles of its hit leaves; `done` is set when no node groups
+// remain (or, for any-hit queries, at the first hit).
+struct TravState
 {
-    int triHit = -1;
-    primHit = 0x7fffffff;
-    tHit = tfar;
-    uHit = 0.f;
-    vHit = 0.f;
-    if (!sc.hasRoot) return -1;
+    uint2 ng;       // current node group: {child base, hit bits 24..31 | imask bits 0..7}
+    float tHit;     // closest hit so far (starts at tfar)
+    int primHit;    // original triangle id of the hit (INT_MAX: none)
+    int triHit;     // leaf-order triangle index of the hit (-1: none)
+    float uHit, vHit;
+    bool done;
+};
+
+__device__ __forceinline__ void trav_init(TravState& s, const SceneDev& sc, float tfar, TravStack& st)
+{
+    s.ng = make_uint2(0u, 0x80000000u);   // root group: one internal "child" at base 0
+    s.tHit = tfar;
+    s.primHit = 0x7fffffff;
+    s.triHit = -1;
+    s.uHit = 0.f;
+    s.vHit = 0.f;
+    s.done = !sc.hasRoot;
     st.sp = 0;
-    // root group: one internal "child" at base 0
-    uint2 ng = make_uint2(0u, 0x80000000u);
-    for (;;)
-    {
-        // ng holds at least one node bit here
-        uint32_t b = 31u - __clz(ng.y & 0xff000000u);
-        ng.y &= ~(1u << b);
-        uint32_t slot = (b - 24u) ^ r.octinv;
-        uint32_t rel = __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
-        uint32_t nodeIdx = ng.x + rel;
-        if (ng.y & 0xff000000u) st.push(ng);
-        const uint4* qp = reinterpret_cast<const uint4*>(sc.nodes + nodeIdx);
-        uint4 q[5];
+}
+
+template <bool anyHit>
+__device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, const TravRay& r, float tnear, TravStack& st)
+{
+    uint2 ng = s.ng;
+    // ng holds at least one node bit here
+    uint32_t b = 31u - __clz(ng.y & 0xff000000u);
+    ng.y &= ~(1u << b);
+    uint32_t slot = (b - 24u) ^ r.octinv;
+    uint32_t rel = __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
+    uint32_t nodeIdx = ng.x + rel;
+    if (ng.y & 0xff000000u) st.push(ng);
+    const uint4* qp = reinterpret_cast<const uint4*>(sc.nodes + nodeIdx);
+    uint4 q[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
-        if (nodeCount) ++*nodeCount;
-        uint32_t hits = node_hits(r, q, tnear, tHit);
-        ng = make_uint2(q[1].x, (hits & 0xff000000u) | (q[0].w >> 24));
-        uint32_t tbits = hits & 0x00ffffffu;
-        uint32_t tbase = q[1].y;
-        while (tbits)
+    for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
+    uint32_t hits = node_hits(r, q, tnear, s.tHit);
+    ng = make_uint2(q[1].x, (hits & 0xff000000u) | (q[0].w >> 24));
+    uint32_t tbits = hits & 0x00ffffffu;
+    uint32_t tbase = q[1].y;
+    while (tbits)
+    {
+        uint32_t tb = 31u - __clz(tbits);
+        tbits &= ~(1u << tb);
+        int ti = (int)(tbase + tb);
+        const float4* tp = reinterpret_cast<const float4*>(sc.tris + ti);
+        float4 a = __ldg(tp), bq = __ldg(tp + 1), c = __ldg(tp + 2);
+        int prim = __float_as_int(a.w);
+        float t, u, v;
+        if (tri_test(r, f3(a.x, a.y, a.z), f3(bq.x, bq.y, bq.z), f3(c.x, c.y, c.z), tnear, s.tHit, prim, s.primHit,
+                     t, u, v))
         {
-            uint32_t tb = 31u - __clz(tbits);
-            tbits &= ~(1u << tb);
-            int ti = (int)(tbase + tb);
-            const float4* tp = reinterpret_cast<const float4*>(sc.tris + ti);
-            float4 a = __ldg(tp), bq = __ldg(tp + 1), c = __ldg(tp + 2);
-            int prim = __float_as_int(a.w);
-            float t, u, v;
-            if (tri_test(r, f3(a.x, a.y, a.z), f3(bq.x, bq.y, bq.z), f3(c.x, c.y, c.z), tnear, tHit, prim, primHit, t,
-                         u, v))
+            s.tHit = t;
+            s.primHit = prim;
+            s.uHit = u;
+            s.vHit = v;
+            s.triHit = ti;
+            if (anyHit)
             {
-                tHit = t;
-                primHit = prim;
-                uHit = u;
-                vHit = v;
-                triHit = ti;
-                if (anyHit) return triHit;
+                s.done = true;
+                return;
             }
         }
-        if (!(ng.y & 0xff000000u))
-        {
-            if (st.sp == 0) break;
-            ng = st.pop();
-        }
     }
-    return triHit;
+    if (!(ng.y & 0xff000000u))
+    {
+        if (st.sp == 0)
+        {
+            s.done = true;
+            return;
+        }
+        ng = st.pop();
+    }
+    s.ng = ng;
+}
+
+// Closest hit (anyHit = false) or any hit (anyHit = true) over (tnear, tfar].
+// Returns the leaf-order triangle index of the hit (or -1), with t/u/v/prim.
+template <bool anyHit>
+__device__ __forceinline__ int traverse(const SceneDev& sc, const TravRay& r, float tnear, float tfar, TravStack& st,
+                                        float& tHit, int& primHit, float& uHit, float& vHit)
+{
+    TravState s;
+    trav_init(s, sc, tfar, st);
+    while (!s.done) trav_step<anyHit>(s, sc, r, tnear, st);
+    tHit = s.tHit;
+    primHit = s.primHit;
+    uHit = s.uHit;
+    vHit = s.vHit;
+    return s.triHit;
 }
 
 // Post-intersection shading and the diffuse bounce

@@ -49,18 +49,36 @@ __device__ __forceinline__ int warp_append(bool pred, int* counter)
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// Lanes refill once at least this many of a warp's 32 lanes are idle
+// (persistent threads with dynamic ray fetch, Aila & Laine, HPG 2009).
+constexpr int kRefillMin = 12;
+
+// Minimum resident 128-thread blocks per SM requested from the compiler for
+// the bounce kernel (8 caps it at 64 registers per thread).
+#ifndef PRT_BOUNCE_MIN_BLOCKS
+#define PRT_BOUNCE_MIN_BLOCKS 8
+#endif
+
 // One bounce of the wavefront over the queue of paths entering `depth`.
 // kFirst: the queue is implicit — item i is (pass, 8x8 tile, Morton index)
 // and the primary ray is generated in registers.
+//
+// Each warp keeps 32 rays in flight.  Traversal advances one 8-wide node per
+// step; as soon as kRefillMin lanes have finished, the finished lanes shade
+// their hit (or accumulate), append survivors to the next queue with one
+// atomic per warp, and fetch fresh rays, so a few long rays do not idle the
+// rest of the warp.
 template <bool kFirst, bool kAlbedo>
-__global__ void __launch_bounds__(256) k_bounce(WaveArgs a, int depth)
+__global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs a, int depth)
 {
     extern __shared__ uint2 s_stack[];
     TravStack st;
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
-    const int lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned ltMask = (1u << lane) - 1u;
     const int W = a.cam.width, H = a.cam.height;
     const int perPass = a.tilesX * a.tilesY * 64;
     int total;
@@ -78,80 +96,113 @@ __global__ void __launch_bounds__(256) k_bounce(WaveArgs a, int depth)
         atomicAdd(a.rays, kFirst ? (unsigned long long)a.passes * (unsigned long long)W * (unsigned long long)H
                                  : (unsigned long long)total);
     const bool final = depth == a.maxDepth;
+
+    bool has = false;         // this lane holds a ray
+    bool exhausted = false;   // warp-uniform: every queue entry has been claimed
+    int pixel = 0;
+    uint32_t rng = 0;
+    float thr = 0.f;
+    TravRay r;
+    TravState ts;
+    ts.done = true;
     for (;;)
     {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(&a.fetch[depth], 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= total) break;
-        const int i = base + lane;
-        bool active = i < total;
-        float3 org = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f);
-        int pixel = 0;
-        uint32_t rng = 0;
-        float thr = kAlbedo ? 1.0f : a.thrConst;
-        if (active)
+        // --- refill idle lanes ---------------------------------------------
+        unsigned idle = __ballot_sync(FULL, !has);
+        if (!exhausted && (__popc(idle) >= kRefillMin || idle == FULL))
         {
-            if (kFirst)
+            int n = __popc(idle);
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&a.fetch[depth], n);
+            base = __shfl_sync(FULL, base, 0);
+            if (base + n >= total) exhausted = true;
+            int i = base + __popc(idle & ltMask);
+            if (!has && i < total)
             {
-                int pass = i / perPass;
-                int r = i - pass * perPass;
-                int tile = r >> 6;
-                int mx, my;
-                morton8x8(r & 63, mx, my);
-                int x = (tile % a.tilesX) * 8 + mx;
-                int y = (tile / a.tilesX) * 8 + my;
-                if (x >= W || y >= H)
+                float3 org, dir;
+                bool ok = true;
+                if (kFirst)
                 {
-                    active = false;
+                    int pass = i / perPass;
+                    int rr = i - pass * perPass;
+                    int tile = rr >> 6;
+                    int mx, my;
+                    morton8x8(rr & 63, mx, my);
+                    int x = (tile % a.tilesX) * 8 + mx;
+                    int y = (tile / a.tilesX) * 8 + my;
+                    if (x >= W || y >= H)
+                    {
+                        ok = false;
+                    }
+                    else
+                    {
+                        pixel = x + y * W;
+                        rng = rng_seed(pass0 + pass, pixel);
+                        camera_ray(a.cam, x, y, rng, org, dir);
+                        thr = kAlbedo ? 1.0f : a.thrConst;
+                    }
                 }
                 else
                 {
-                    pixel = x + y * W;
-                    rng = rng_seed(pass0 + pass, pixel);
-                    camera_ray(a.cam, x, y, rng, org, dir);
+                    PathRec pr = load_path(a.qin, i);
+                    org = f3(pr.w0.x, pr.w0.y, pr.w0.z);
+                    pixel = __float_as_int(pr.w0.w);
+                    dir = f3(pr.w1.x, pr.w1.y, pr.w1.z);
+                    rng = __float_as_uint(pr.w1.w);
+                    thr = kAlbedo ? __ldcs(a.thrIn + i) : a.thrConst;
+                }
+                if (ok)
+                {
+                    has = true;
+                    trav_setup(r, org, dir);
+                    trav_init(ts, a.scene, FLT_MAX, st);
                 }
             }
-            else
-            {
-                PathRec pr = load_path(a.qin, i);
-                org = f3(pr.w0.x, pr.w0.y, pr.w0.z);
-                pixel = __float_as_int(pr.w0.w);
-                dir = f3(pr.w1.x, pr.w1.y, pr.w1.z);
-                rng = __float_as_uint(pr.w1.w);
-                if (kAlbedo) thr = __ldcs(a.thrIn + i);
-            }
         }
+        if (__ballot_sync(FULL, has) == 0)
+        {
+            if (exhausted) break;
+            continue;
+        }
+        // --- traverse until the warp has enough idle lanes ------------------
+        for (;;)
+        {
+            if (has && !ts.done) trav_step<false>(ts, a.scene, r, 0.0f, st);
+            unsigned running = __ballot_sync(FULL, has && !ts.done);
+            if (running == 0) break;
+            if (!exhausted && 32 - __popc(running) >= kRefillMin) break;
+        }
+        // --- finish the lanes whose traversal is complete ---------------------
+        const bool fin = has && ts.done;
         bool cont = false;
         float contrib = 0.f;
-        if (active)
+        if (fin)
         {
-            TravRay r;
-            trav_setup(r, org, dir);
-            float t, u, v;
-            int prim;
-            int ti = traverse<false>(a.scene, r, 0.0f, FLT_MAX, st, t, prim, u, v);
-            if (ti < 0)
+            if (ts.triHit < 0)
             {
                 contrib = __fmul_rn(thr, a.sky);
             }
             else if (!final)
             {
-                if (kAlbedo) thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + prim) : 0.8f);
-                diffuse_bounce(a.scene.tris, ti, org, dir, t, rng);
+                if (kAlbedo) thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + ts.primHit) : 0.8f);
+                float3 org = r.org, dir = r.dir;
+                diffuse_bounce(a.scene.tris, ts.triHit, org, dir, ts.tHit, rng);
+                r.org = org;
+                r.dir = dir;
                 cont = true;
             }
         }
         int o = warp_append(cont, &a.counts[depth + 1]);
         if (cont)
         {
-            store_path(a.qout, o, org, pixel, dir, rng);
+            store_path(a.qout, o, r.org, pixel, r.dir, rng);
             if (kAlbedo) __stcs(a.thrOut + o, thr);
         }
-        else if (active)
+        else if (fin)
         {
             red_add_v4(a.accum + pixel, contrib, contrib, contrib, 1.0f);
         }
+        if (fin) has = false;
     }
 }
 

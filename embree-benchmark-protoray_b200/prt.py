@@ -17,7 +17,9 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libprt_b200.so")
+# PRT_B200_LIB selects another build of the same library (e.g. a variant
+# compiled with different launch bounds); the default is the in-tree build.
+LIB_PATH = os.environ.get("PRT_B200_LIB", os.path.join(HERE, "libprt_b200.so"))
 
 PRT_OK, PRT_EINVAL, PRT_ENOMEM, PRT_ECUDA, PRT_ETIMEOUT, PRT_EINTERNAL, PRT_EIO, PRT_ESTATE = range(8)
 STATUS_NAMES = {0: "PRT_OK", 1: "PRT_EINVAL", 2: "PRT_ENOMEM", 3: "PRT_ECUDA", 4: "PRT_ETIMEOUT",

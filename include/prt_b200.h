@@ -106,7 +106,7 @@ typedef struct {
 
 /* Autotuned launch configuration. */
 typedef struct {
-    int blockSize;        /* threads per block of the bounce kernel */
+    int blockSize;        /* threads per block of the bounce kernel (32..128) */
     int blocksPerSM;      /* resident blocks per SM of the persistent grid */
     int pathsPerWave;     /* queue capacity (paths in flight per wave) */
     double mray;          /* throughput measured for the winner */

@@ -1131,3 +1131,24 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
 }
 
 } // extern "C"
+
+namespace prt_b200 {
+
+// Read-only view of a context for prt_render_noalloc (noalloc.cu).
+int ctx_noalloc_view(prt_ctx* ctx, SceneDev* scene, int* device, cudaStream_t* stream, int* numSMs, LaunchCfg* cfg,
+                     float* sky, bool* albedo)
+{
+    if (!ctx->built) return fail(ctx, PRT_ESTATE, "acceleration structure not built (prt_build_accel)");
+    *scene = scene_dev(ctx);
+    *device = ctx->device;
+    *stream = ctx->stream;
+    *numSMs = ctx->numSMs;
+    *cfg = ctx->cfg;
+    *sky = ctx->sky;
+    *albedo = ctx->dAlbedo != nullptr;
+    return PRT_OK;
+}
+
+int ctx_fail(prt_ctx* ctx, int status, const char* msg) { return fail(ctx, status, msg); }
+
+} // namespace prt_b200

@@ -33,7 +33,7 @@ EXPORTS = [
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
-    "prt_render_batch", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_launch_count",
+    "prt_render_batch", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
 ]
 
 
@@ -121,6 +121,7 @@ def lib() -> C.CDLL:
         "prt_autotune": (ip, [vp, ip, ip, C.POINTER(Tune)]),
         "prt_set_tune": (ip, [vp, C.POINTER(Tune)]),
         "prt_get_tune": (ip, [vp, C.POINTER(Tune)]),
+        "prt_render_noalloc": (ip, [vp, C.POINTER(Camera), ip, ip, ip, ip, ip, vp, C.POINTER(C.c_longlong)]),
         "prt_launch_count": (C.c_longlong, [vp]),
     }
     for name, (res, args) in sig.items():
@@ -293,6 +294,15 @@ class Context:
     def set_tune(self, block: int, per_sm: int, paths_per_wave: int):
         t = Tune(block, per_sm, paths_per_wave, 0.0)
         self._check(self.L.prt_set_tune(self.h, C.byref(t)), "prt_set_tune")
+
+    def render_noalloc(self, cam: Camera, width: int, height: int, pass0: int, spp: int, max_depth: int,
+                       accum_dev) -> int:
+        """Allocation-free render into a caller-owned device buffer (see
+        prt_render_noalloc in include/prt_b200.h); returns the ray count."""
+        rays = C.c_longlong(0)
+        self._check(self.L.prt_render_noalloc(self.h, C.byref(cam), width, height, pass0, spp, max_depth,
+                                              _ptr(accum_dev), C.byref(rays)), "prt_render_noalloc")
+        return rays.value
 
     def launch_count(self) -> int:
         return int(self.L.prt_launch_count(self.h))

@@ -201,6 +201,22 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best);
 int prt_set_tune(prt_ctx* ctx, const prt_tune* tune);
 int prt_get_tune(prt_ctx* ctx, prt_tune* tune);
 
+/* --- rendering without device allocation (no counterpart in the reference) --- */
+/* Renders passes [pass0, pass0+spp) of ctx's built scene through `cam` into
+ * the caller's device buffer `accum` (width*height*4 floats: sum r, g, b,
+ * weight; added to, not cleared) and returns the closest-hit query count in
+ * `rays` (nullable).  It allocates nothing: for callers that cannot allocate
+ * device memory at render time (an application that owns the GPU's memory
+ * through its own pool, or a frame loop that cannot afford cudaMalloc's
+ * implicit synchronisation).  Its path queues live in one fixed 36 MiB device
+ * array per GPU, so frames are limited to 524288 pixels after rounding up to
+ * 8x8 tiles (larger ones return PRT_EINVAL).  All calls on a device share that
+ * array: calls that overlap on the GPU race, so serialise them.  The first
+ * call on a device resolves the array's address; make it before any stream
+ * capture. */
+int prt_render_noalloc(prt_ctx* ctx, const prt_camera* cam, int width, int height, int pass0, int spp, int maxDepth,
+                       float* accum, long long* rays);
+
 /* Kernel launches issued by this context since creation (for accounting). */
 long long prt_launch_count(prt_ctx* ctx);
 

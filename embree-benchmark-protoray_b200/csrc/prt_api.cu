@@ -876,8 +876,10 @@ int prt_render_replay(prt_ctx* ctx, int pass0, int spp, int maxDepth, prt_render
     CK(cudaSetDevice(ctx->device));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+    CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(unsigned long long), ctx->stream));
     ctx->launches += launch_replay(scene_dev(ctx), camera_dev(ctx->cam, ctx->W, ctx->H), ctx->dAccum, pass0, spp,
-                                   maxDepth, ctx->sky, nullptr, nullptr, nullptr, ctx->dRays, false, ctx->stream);
+                                   maxDepth, ctx->sky, nullptr, nullptr, nullptr, ctx->dRays, ctx->dFetch, false,
+                                   ctx->numSMs, ctx->stream);
     CK(cudaGetLastError());
     return finish_stats(ctx, stats, spp);
 }
@@ -908,8 +910,10 @@ int prt_render_backward(prt_ctx* ctx, int pass0, int spp, int maxDepth, const fl
     else CK(cudaMalloc(&gS, sizeof(float)));
     CK(cudaMemsetAsync(gA, 0, sizeof(float) * (size_t)ctx->nt, ctx->stream));
     CK(cudaMemsetAsync(gS, 0, sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(unsigned long long), ctx->stream));
     ctx->launches += launch_replay(scene_dev(ctx), camera_dev(ctx->cam, ctx->W, ctx->H), ctx->dAccum, pass0, spp,
-                                   maxDepth, ctx->sky, gL, gA, gS, nullptr, true, ctx->stream);
+                                   maxDepth, ctx->sky, gL, gA, gS, nullptr, ctx->dFetch, true, ctx->numSMs,
+                                   ctx->stream);
     CK(cudaGetLastError());
     if (!devA) CK(cudaMemcpyAsync(d_albedo, gA, sizeof(float) * (size_t)ctx->nt, cudaMemcpyDeviceToHost, ctx->stream));
     if (!devS) CK(cudaMemcpyAsync(d_sky, gS, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1045,6 +1049,21 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
             else ++it;
     }
     return st;
+}
+
+int prt_read_accel(prt_ctx* ctx, void* nodes, int nodeCapacity, void* tris, int triCapacity, int* nodeCount,
+                   int* triCount)
+{
+    int st = check_ready(ctx, false);
+    if (st != PRT_OK) return st;
+    if (nodeCount) *nodeCount = ctx->bvh.nodeCount;
+    if (triCount) *triCount = ctx->bvh.triCount;
+    CK(cudaSetDevice(ctx->device));
+    if (nodes && nodeCapacity >= ctx->bvh.nodeCount && ctx->bvh.nodeCount > 0)
+        CK(cudaMemcpy(nodes, ctx->bvh.nodes, sizeof(Bvh8Node) * (size_t)ctx->bvh.nodeCount, cudaMemcpyDeviceToHost));
+    if (tris && triCapacity >= ctx->bvh.triCount && ctx->bvh.triCount > 0)
+        CK(cudaMemcpy(tris, ctx->bvh.tris, sizeof(TriRec) * (size_t)ctx->bvh.triCount, cudaMemcpyDeviceToHost));
+    return PRT_OK;
 }
 
 int prt_set_tune(prt_ctx* ctx, const prt_tune* t)

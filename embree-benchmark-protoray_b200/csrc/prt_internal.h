@@ -104,9 +104,10 @@ int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n
 int launch_resolve_ldr(const float4* accum, uint32_t* out, int n, cudaStream_t s);
 int launch_advance_pass(int* passBase, int spp, cudaStream_t s);
 int launch_query(const SceneDev& sc, const RayRec* ray, HitRec* hit, float* pNg, cudaStream_t s);
+// fetch: a zeroed 64-bit work counter on the device
 int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int pass0, int spp, int maxDepth, float sky,
-                  const float* dL, float* dAlbedo, float* dSky, unsigned long long* rays, bool backward,
-                  cudaStream_t s);
+                  const float* dL, float* dAlbedo, float* dSky, unsigned long long* rays, int* fetch, bool backward,
+                  int numSMs, cudaStream_t s);
 int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s);
 int launch_fill(float4* p, size_t n, cudaStream_t s);
 

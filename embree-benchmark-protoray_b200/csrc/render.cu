@@ -286,84 +286,137 @@ __global__ void k_advance_pass(int* passBase, int spp) { *passBase += spp; }
 
 constexpr int kReplayMaxDepth = 16;
 
-// Path-replay megakernel: one thread per (pass, pixel) path.  The forward
-// mode accumulates the path's radiance; the backward mode re-traces the same
-// path from its seed and scatters dL/d(radiance) into the albedo of every
-// triangle the path bounced off and into the sky radiance:
+// Path-replay megakernel: each lane carries whole paths (pass, pixel), from
+// the camera ray to escape or maxDepth.  The forward mode accumulates the
+// path's radiance; the backward mode re-traces the same path from its seed
+// and scatters dL/d(radiance) into the albedo of every triangle the path
+// bounced off and into the sky radiance:
 //   radiance = sky * prod_k albedo[prim_k]
 //   d radiance / d albedo[prim_k] = radiance / albedo[prim_k]
 //   d radiance / d sky            = prod_k albedo[prim_k]
+// Paths are regenerated per lane (a lane whose path ends takes the next one
+// once kRefillMin lanes of its warp are free), and traversal advances one node
+// per step, as in k_bounce.  The bounce arithmetic is the same device code as
+// the wavefront renderer's, so both compute bit-identical paths.
 template <bool kBackward>
-__global__ void __launch_bounds__(128) k_replay(SceneDev sc, CameraDev cam, float4* accum, int pass0, int spp,
-                                                int maxDepth, float sky, const float* __restrict__ dL,
-                                                float* dAlbedo, float* dSky, unsigned long long* rays)
+__global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, float4* accum, int pass0, int spp,
+                                                   int maxDepth, float sky, const float* __restrict__ dL,
+                                                   float* dAlbedo, float* dSky, unsigned long long* rays,
+                                                   int* fetch)
 {
     extern __shared__ uint2 s_stack[];
     TravStack st;
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned ltMask = (1u << lane) - 1u;
     const int W = cam.width, H = cam.height;
-    const long long total = (long long)spp * W * H;
+    const long long npix = (long long)W * H;
+    const long long total = (long long)spp * npix;
     float skyGrad = 0.f;
     unsigned long long myRays = 0;
-    for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < total;
-         gi += (long long)gridDim.x * blockDim.x)
+
+    bool has = false;
+    bool exhausted = false;
+    int pixel = 0, depth = 0, np = 0;
+    uint32_t rng = 0;
+    float thr = 1.f, g = 0.f;
+    int prims[kBackward ? kReplayMaxDepth : 1];
+    TravRay r;
+    TravState ts;
+    ts.done = true;
+    for (;;)
     {
-        int pass = (int)(gi / ((long long)W * H));
-        int pixel = (int)(gi - (long long)pass * W * H);
-        int x = pixel % W, y = pixel / W;
-        float g = 0.f;
-        if (kBackward)
+        unsigned idle = __ballot_sync(FULL, !has);
+        if (!exhausted && (__popc(idle) >= kRefillMin || idle == FULL))
         {
-            g = dL[3 * (size_t)pixel] + dL[3 * (size_t)pixel + 1] + dL[3 * (size_t)pixel + 2];
-            if (g == 0.f) continue;
-        }
-        uint32_t rng = rng_seed(pass0 + pass, pixel);
-        float3 org, dir;
-        camera_ray(cam, x, y, rng, org, dir);
-        float thr = 1.0f;
-        int prims[kReplayMaxDepth];
-        int np = 0;
-        bool escaped = false;
-        for (int depth = 0;; ++depth)
-        {
-            TravRay r;
-            trav_setup(r, org, dir);
-            float t, u, v;
-            int prim;
-            int ti = traverse<false>(sc, r, 0.0f, FLT_MAX, st, t, prim, u, v);
-            ++myRays;
-            if (ti < 0) { escaped = true; break; }
-            if (depth == maxDepth) break;
-            thr = __fmul_rn(thr, sc.albedo ? __ldg(sc.albedo + prim) : 0.8f);
-            if (kBackward) prims[np++] = prim;
-            diffuse_bounce(sc.tris, ti, org, dir, t, rng);
-        }
-        float c = escaped ? __fmul_rn(thr, sky) : 0.0f;
-        if (!kBackward)
-        {
-            red_add_v4(accum + pixel, c, c, c, 1.0f);
-        }
-        else if (escaped)
-        {
-            skyGrad += g * thr;
-            float gc = g * c;
-            for (int k = 0; k < np; ++k)
+            int n = __popc(idle);
+            long long base = 0;
+            if (lane == 0) base = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(fetch), (unsigned long long)n);
+            base = __shfl_sync(FULL, base, 0);
+            if (base + n >= total) exhausted = true;
+            long long gi = base + __popc(idle & ltMask);
+            if (!has && gi < total)
             {
-                float a = sc.albedo ? __ldg(sc.albedo + prims[k]) : 0.8f;
-                atomicAdd(dAlbedo + prims[k], gc / a);
+                int pass = (int)(gi / npix);
+                pixel = (int)(gi - (long long)pass * npix);
+                bool ok = true;
+                if (kBackward)
+                {
+                    g = dL[3 * (size_t)pixel] + dL[3 * (size_t)pixel + 1] + dL[3 * (size_t)pixel + 2];
+                    ok = g != 0.f;
+                }
+                if (ok)
+                {
+                    rng = rng_seed(pass0 + pass, pixel);
+                    float3 org, dir;
+                    camera_ray(cam, pixel % W, pixel / W, rng, org, dir);
+                    trav_setup(r, org, dir);
+                    trav_init(ts, sc, FLT_MAX, st);
+                    thr = 1.0f;
+                    depth = 0;
+                    np = 0;
+                    has = true;
+                }
+            }
+        }
+        if (__ballot_sync(FULL, has) == 0)
+        {
+            if (exhausted) break;
+            continue;
+        }
+        for (;;)
+        {
+            if (has && !ts.done) trav_step<false>(ts, sc, r, 0.0f, st);
+            unsigned running = __ballot_sync(FULL, has && !ts.done);
+            if (running == 0) break;
+            if (32 - __popc(running) >= kRefillMin) break;
+        }
+        if (has && ts.done)
+        {
+            ++myRays;
+            bool escaped = ts.triHit < 0;
+            if (!escaped && depth < maxDepth)
+            {
+                // continue the path in this lane
+                thr = __fmul_rn(thr, sc.albedo ? __ldg(sc.albedo + ts.primHit) : 0.8f);
+                if (kBackward) prims[np++] = ts.primHit;
+                float3 org = r.org, dir = r.dir;
+                diffuse_bounce(sc.tris, ts.triHit, org, dir, ts.tHit, rng);
+                trav_setup(r, org, dir);
+                trav_init(ts, sc, FLT_MAX, st);
+                ++depth;
+            }
+            else
+            {
+                float c = escaped ? __fmul_rn(thr, sky) : 0.0f;
+                if (!kBackward)
+                {
+                    red_add_v4(accum + pixel, c, c, c, 1.0f);
+                }
+                else if (escaped)
+                {
+                    skyGrad += g * thr;
+                    float gc = g * c;
+                    for (int k = 0; k < np; ++k)
+                    {
+                        float al = sc.albedo ? __ldg(sc.albedo + prims[k]) : 0.8f;
+                        atomicAdd(dAlbedo + prims[k], gc / al);
+                    }
+                }
+                has = false;
             }
         }
     }
-    // warp-reduce the counters, one atomic per warp
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
     {
-        skyGrad += __shfl_down_sync(0xffffffffu, skyGrad, off);
-        myRays += __shfl_down_sync(0xffffffffu, myRays, off);
+        skyGrad += __shfl_down_sync(FULL, skyGrad, off);
+        myRays += __shfl_down_sync(FULL, myRays, off);
     }
-    if ((threadIdx.x & 31) == 0)
+    if (lane == 0)
     {
         if (kBackward && skyGrad != 0.f) atomicAdd(dSky, skyGrad);
         if (rays) atomicAdd(rays, myRays);
@@ -373,118 +426,146 @@ __global__ void __launch_bounds__(128) k_replay(SceneDev sc, CameraDev cam, floa
 // Batched bounce: the paths of many requests share one queue.  Item i of the
 // first bounce is a global path index resolved to (request, pass, tile,
 // Morton index) by a binary search over the requests' path ranges; later
-// bounces carry (request << 24 | pixel) in the path record.
+// bounces carry (request << 24 | pixel) in the path record.  Lanes refill
+// dynamically as in k_bounce.
 template <bool kFirst>
-__global__ void __launch_bounds__(256) k_batch_bounce(BatchArgs a, int depth)
+__global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
 {
     extern __shared__ uint2 s_dyn[];
     uint2* s_stack = s_dyn;
     long long* s_begin = reinterpret_cast<long long*>(s_dyn + kShared * blockDim.x);
-    for (int r = threadIdx.x; r < a.nreq; r += blockDim.x) s_begin[r] = a.reqs[r].pathBegin;
+    for (int q = threadIdx.x; q < a.nreq; q += blockDim.x) s_begin[q] = a.reqs[q].pathBegin;
     __syncthreads();
     TravStack st;
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
-    const int lane = threadIdx.x & 31;
-    long long total = kFirst ? (a.waveEnd - a.waveBegin) : (long long)*(volatile int*)&a.counts[depth];
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned ltMask = (1u << lane) - 1u;
+    const long long total = kFirst ? (a.waveEnd - a.waveBegin) : (long long)*(volatile int*)&a.counts[depth];
     if (!kFirst && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.rays, (unsigned long long)total);
     unsigned long long myRays = 0;
+    float thrDepth = 1.0f;
+    for (int d = 0; d < depth; ++d) thrDepth = __fmul_rn(thrDepth, 0.8f);
+
+    bool has = false;
+    bool exhausted = false;
+    int pixel = 0, req = 0;
+    uint32_t rng = 0;
+    TravRay r;
+    TravState ts;
+    ts.done = true;
     for (;;)
     {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(&a.fetch[depth], 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= total) break;
-        const int i = base + lane;
-        bool active = i < total;
-        float3 org = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f);
-        int pixel = 0, req = 0;
-        uint32_t rng = 0;
-        if (active)
+        unsigned idle = __ballot_sync(FULL, !has);
+        if (!exhausted && (__popc(idle) >= kRefillMin || idle == FULL))
         {
-            if (kFirst)
+            int n = __popc(idle);
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&a.fetch[depth], n);
+            base = __shfl_sync(FULL, base, 0);
+            if (base + n >= total) exhausted = true;
+            int i = base + __popc(idle & ltMask);
+            if (!has && i < total)
             {
-                long long gi = a.waveBegin + i;
-                int lo = 0, hi = a.nreq - 1;
-                while (lo < hi)
+                float3 org, dir;
+                bool ok = true;
+                if (kFirst)
                 {
-                    int mid = (lo + hi + 1) >> 1;
-                    if (s_begin[mid] <= gi) lo = mid;
-                    else hi = mid - 1;
-                }
-                req = lo;
-                const BatchReq& R = a.reqs[req];
-                long long local = gi - R.pathBegin;
-                int perPass = R.tilesX * R.tilesY * 64;
-                int pass = (int)(local / perPass);
-                int rr = (int)(local - (long long)pass * perPass);
-                int tile = rr >> 6;
-                int mx, my;
-                morton8x8(rr & 63, mx, my);
-                int x = (tile % R.tilesX) * 8 + mx;
-                int y = (tile / R.tilesX) * 8 + my;
-                if (x >= R.cam.width || y >= R.cam.height)
-                {
-                    active = false;
+                    long long gi = a.waveBegin + i;
+                    int lo = 0, hi = a.nreq - 1;
+                    while (lo < hi)
+                    {
+                        int mid = (lo + hi + 1) >> 1;
+                        if (s_begin[mid] <= gi) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    req = lo;
+                    const BatchReq& R = a.reqs[req];
+                    long long local = gi - s_begin[req];
+                    int perPass = R.tilesX * R.tilesY * 64;
+                    int pass = (int)(local / perPass);
+                    int rr = (int)(local - (long long)pass * perPass);
+                    int tile = rr >> 6;
+                    int mx, my;
+                    morton8x8(rr & 63, mx, my);
+                    int x = (tile % R.tilesX) * 8 + mx;
+                    int y = (tile / R.tilesX) * 8 + my;
+                    if (x >= R.cam.width || y >= R.cam.height)
+                    {
+                        ok = false;
+                    }
+                    else
+                    {
+                        pixel = x + y * R.cam.width;
+                        rng = rng_seed(pass, pixel);
+                        camera_ray(R.cam, x, y, rng, org, dir);
+                        ++myRays;
+                    }
                 }
                 else
                 {
-                    pixel = x + y * R.cam.width;
-                    rng = rng_seed(pass, pixel);
-                    camera_ray(R.cam, x, y, rng, org, dir);
-                    ++myRays;
+                    PathRec pr = load_path(a.qin, i);
+                    org = f3(pr.w0.x, pr.w0.y, pr.w0.z);
+                    int tag = __float_as_int(pr.w0.w);
+                    req = (int)((uint32_t)tag >> 24);
+                    pixel = tag & 0xffffff;
+                    dir = f3(pr.w1.x, pr.w1.y, pr.w1.z);
+                    rng = __float_as_uint(pr.w1.w);
+                }
+                if (ok)
+                {
+                    has = true;
+                    trav_setup(r, org, dir);
+                    trav_init(ts, a.reqs[req].scene, FLT_MAX, st);
                 }
             }
-            else
-            {
-                PathRec pr = load_path(a.qin, i);
-                org = f3(pr.w0.x, pr.w0.y, pr.w0.z);
-                int tag = __float_as_int(pr.w0.w);
-                req = (int)((uint32_t)tag >> 24);
-                pixel = tag & 0xffffff;
-                dir = f3(pr.w1.x, pr.w1.y, pr.w1.z);
-                rng = __float_as_uint(pr.w1.w);
-            }
         }
+        if (__ballot_sync(FULL, has) == 0)
+        {
+            if (exhausted) break;
+            continue;
+        }
+        for (;;)
+        {
+            if (has && !ts.done) trav_step<false>(ts, a.reqs[req].scene, r, 0.0f, st);
+            unsigned running = __ballot_sync(FULL, has && !ts.done);
+            if (running == 0) break;
+            if (!exhausted && 32 - __popc(running) >= kRefillMin) break;
+        }
+        const bool fin = has && ts.done;
         bool cont = false;
         float contrib = 0.f;
-        float4* accum = nullptr;
-        if (active)
+        if (fin)
         {
             const BatchReq& R = a.reqs[req];
-            accum = R.accum;
-            TravRay r;
-            trav_setup(r, org, dir);
-            float t, u, v;
-            int prim;
-            int ti = traverse<false>(R.scene, r, 0.0f, FLT_MAX, st, t, prim, u, v);
-            if (ti < 0)
+            if (ts.triHit < 0)
             {
-                float thr = 1.0f;
-                for (int d = 0; d < depth; ++d) thr = __fmul_rn(thr, 0.8f);
-                contrib = __fmul_rn(thr, a.sky);
+                contrib = __fmul_rn(thrDepth, a.sky);
             }
             else if (depth < R.maxDepth)
             {
-                diffuse_bounce(R.scene.tris, ti, org, dir, t, rng);
+                float3 org = r.org, dir = r.dir;
+                diffuse_bounce(R.scene.tris, ts.triHit, org, dir, ts.tHit, rng);
+                r.org = org;
+                r.dir = dir;
                 cont = true;
             }
         }
         int o = warp_append(cont, &a.counts[depth + 1]);
-        if (cont) store_path(a.qout, o, org, (req << 24) | pixel, dir, rng);
-        else if (active) red_add_v4(accum + pixel, contrib, contrib, contrib, 1.0f);
+        if (cont) store_path(a.qout, o, r.org, (req << 24) | pixel, r.dir, rng);
+        else if (fin) red_add_v4(a.reqs[req].accum + pixel, contrib, contrib, contrib, 1.0f);
+        if (fin) has = false;
     }
     if (kFirst)
     {
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) myRays += __shfl_down_sync(0xffffffffu, myRays, off);
+        for (int off = 16; off > 0; off >>= 1) myRays += __shfl_down_sync(FULL, myRays, off);
         if (lane == 0 && myRays) atomicAdd(a.rays, myRays);
     }
 }
 
-// Persistent grid: cfg.blocksPerSM blocks per SM, capped by (and, when 0,
-// equal to) the number of blocks the kernel can keep resident per SM.
 template <class Kernel>
 int grid_for(Kernel kernel, int block, size_t shmem, int numSMs, const LaunchCfg& cfg)
 {
@@ -563,17 +644,20 @@ int launch_advance_pass(int* passBase, int spp, cudaStream_t s)
 }
 
 int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int pass0, int spp, int maxDepth, float sky,
-                  const float* dL, float* dAlbedo, float* dSky, unsigned long long* rays, bool backward,
-                  cudaStream_t s)
+                  const float* dL, float* dAlbedo, float* dSky, unsigned long long* rays, int* fetch, bool backward,
+                  int numSMs, cudaStream_t s)
 {
     long long total = (long long)spp * cam.width * cam.height;
     if (total <= 0) return 0;
-    int block = 128;
-    long long g = (total + block - 1) / block;
-    int grid = (int)(g < 148LL * 32 ? g : 148LL * 32);
+    const int block = 128;
     size_t shmem = sizeof(uint2) * kShared * block;
-    if (backward) k_replay<true><<<grid, block, shmem, s>>>(sc, cam, accum, pass0, spp, maxDepth, sky, dL, dAlbedo, dSky, rays);
-    else k_replay<false><<<grid, block, shmem, s>>>(sc, cam, accum, pass0, spp, maxDepth, sky, dL, dAlbedo, dSky, rays);
+    LaunchCfg cfg;
+    auto go = [&](auto kernel) {
+        int grid = grid_for(kernel, block, shmem, numSMs, cfg);
+        kernel<<<grid, block, shmem, s>>>(sc, cam, accum, pass0, spp, maxDepth, sky, dL, dAlbedo, dSky, rays, fetch);
+    };
+    if (backward) go(k_replay<true>);
+    else go(k_replay<false>);
     return 1;
 }
 

@@ -33,7 +33,7 @@ EXPORTS = [
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
-    "prt_render_batch", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
+    "prt_render_batch", "prt_read_accel", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
 ]
 
 
@@ -118,6 +118,7 @@ def lib() -> C.CDLL:
         "prt_render_backward": (ip, [vp, ip, ip, ip, vp, vp, vp]),
         "prt_render_replay": (ip, [vp, ip, ip, ip, C.POINTER(RenderStats)]),
         "prt_render_batch": (ip, [vp, C.POINTER(Request), ip, C.POINTER(RenderStats)]),
+        "prt_read_accel": (ip, [vp, vp, ip, vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "prt_autotune": (ip, [vp, ip, ip, C.POINTER(Tune)]),
         "prt_set_tune": (ip, [vp, C.POINTER(Tune)]),
         "prt_get_tune": (ip, [vp, C.POINTER(Tune)]),
@@ -303,6 +304,16 @@ class Context:
         self._check(self.L.prt_render_noalloc(self.h, C.byref(cam), width, height, pass0, spp, max_depth,
                                               _ptr(accum_dev), C.byref(rays)), "prt_render_noalloc")
         return rays.value
+
+    def read_accel(self):
+        """(nodes uint32[N, 20], tris float32[T, 12]) of the built 8-wide BVH."""
+        n, t = C.c_int(), C.c_int()
+        self._check(self.L.prt_read_accel(self.h, None, 0, None, 0, C.byref(n), C.byref(t)), "prt_read_accel")
+        nodes = np.zeros((max(n.value, 1), 20), np.uint32)
+        tris = np.zeros((max(t.value, 1), 12), np.float32)
+        self._check(self.L.prt_read_accel(self.h, nodes.ctypes.data, len(nodes), tris.ctypes.data, len(tris),
+                                          C.byref(n), C.byref(t)), "prt_read_accel")
+        return nodes[: n.value], tris[: t.value]
 
     def launch_count(self) -> int:
         return int(self.L.prt_launch_count(self.h))

@@ -194,6 +194,14 @@ int prt_render_replay(prt_ctx* ctx, int pass0, int spp, int maxDepth, prt_render
  * one persistent kernel per bounce (CUDA-graph captured), on ctx's device. */
 int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_stats* stats);
 
+/* --- inspection --- */
+/* Copies the acceleration structure to host memory: 80-byte 8-wide nodes
+ * and 48-byte leaf triangles (layouts in csrc/prt_device.cuh).  Either
+ * buffer may be NULL; counts (nullable) receive the sizes.  Used by the
+ * structural tests. */
+int prt_read_accel(prt_ctx* ctx, void* nodes, int nodeCapacity, void* tris, int triCapacity, int* nodeCount,
+                   int* triCount);
+
 /* --- launch configuration --- */
 /* Times candidate bounce-kernel configurations on the current scene/frame
  * and keeps the fastest for later renders. */

@@ -1,0 +1,93 @@
+"""Structural checks of the 8-wide BVH built on the GPU: every triangle in
+exactly one leaf, leaf triangles carry their own vertices, child boxes
+enclose their contents, the tree depth fits the traversal stack."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _decode(nodes):
+    """Per node: origin (3), scale (3), imask, child base, tri base, meta[8],
+    qlo[3][8], qhi[3][8]."""
+    q = nodes.view(np.uint32)
+    origin = q[:, 0:3].view(np.float32)
+    e = q[:, 3]
+    scale = np.stack([np.ldexp(1.0, ((e >> (8 * k)) & 0xFF).astype(np.int64) - 127) for k in range(3)], axis=1)
+    imask = (e >> 24) & 0xFF
+    child = q[:, 4].astype(np.int64)
+    tbase = q[:, 5].astype(np.int64)
+    b = nodes.view(np.uint8).reshape(len(nodes), 80)
+    meta = b[:, 24:32]
+    qlo = np.stack([b[:, 32:40], b[:, 40:48], b[:, 48:56]], axis=1)
+    qhi = np.stack([b[:, 56:64], b[:, 64:72], b[:, 72:80]], axis=1)
+    return origin, scale, imask, child, tbase, meta, qlo, qhi
+
+
+@pytest.mark.parametrize("scene", ["small", "batch3", "one", "two"])
+def test_bvh_structure(scene, small):
+    import prt
+    import scenes
+    if scene == "small":
+        mesh, _ = small
+        pos, idx = mesh.positions, mesh.indices
+    elif scene == "batch3":
+        mesh, _ = scenes.batch_scene(3)
+        pos, idx = mesh.positions, mesh.indices
+    elif scene == "one":
+        pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+        idx = np.array([[0, 1, 2]], np.int32)
+    else:
+        pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
+        idx = np.array([[0, 1, 2], [0, 1, 3]], np.int32)
+    c = prt.Context(0)
+    c.load_mesh(idx, pos)
+    st = c.build()
+    nodes, tris = c.read_accel()
+    assert st["levels"] <= 64
+    n = len(idx)
+    prims = tris[:, 3].view(np.int32)
+    assert np.array_equal(np.sort(prims), np.arange(n))
+    # leaf triangles hold their own vertices
+    np.testing.assert_array_equal(tris[:, 0:3], pos[idx[prims, 0]])
+    np.testing.assert_array_equal(tris[:, 4:7], pos[idx[prims, 1]])
+    np.testing.assert_array_equal(tris[:, 8:11], pos[idx[prims, 2]])
+
+    origin, scale, imask, child, tbase, meta, qlo, qhi = _decode(nodes)
+    seen_nodes = np.zeros(len(nodes), np.int64)
+    seen_tris = np.zeros(n, np.int64)
+    seen_nodes[0] += 1
+    for i in range(len(nodes)):
+        rank = 0
+        for s in range(8):
+            m = int(meta[i, s])
+            if m == 0:
+                continue
+            lo = origin[i] + qlo[i, :, s] * scale[i]
+            hi = origin[i] + qhi[i, :, s] * scale[i]
+            eps = 1e-6 * (np.abs(lo) + np.abs(hi) + 1)
+            if (m & 0x1F) >= 24:
+                assert (m & 0x1F) - 24 == s and (imask[i] >> s) & 1
+                ci = child[i] + rank
+                rank += 1
+                seen_nodes[ci] += 1
+                # the child node's own box lies inside the slot box
+                cl = origin[ci]
+                ch = origin[ci] + 255 * scale[ci]
+                used = meta[ci] != 0
+                clo = origin[ci][:, None] + qlo[ci][:, used] * scale[ci][:, None]
+                chi = origin[ci][:, None] + qhi[ci][:, used] * scale[ci][:, None]
+                assert np.all(clo.min(axis=1) >= lo - eps) and np.all(chi.max(axis=1) <= hi + eps + 255 * scale[ci])
+            else:
+                cnt = bin(m >> 5).count("1")
+                assert (m >> 5) == (1 << cnt) - 1 and 1 <= cnt <= 3
+                off = m & 0x1F
+                for k in range(cnt):
+                    t = tbase[i] + off + k
+                    seen_tris[prims[t]] += 1
+                    v = tris[t].reshape(3, 4)[:, :3]
+                    assert np.all(v >= lo - eps) and np.all(v <= hi + eps)
+        assert rank == bin(int(imask[i])).count("1")
+    assert np.all(seen_nodes == 1)
+    assert np.all(seen_tris == 1)

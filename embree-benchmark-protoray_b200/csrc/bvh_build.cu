@@ -699,7 +699,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
             status = PRT_EINTERNAL;
             goto done;
         }
-        if (levels > kStackMax)
+        if (2 * levels > kStackMax)
         {
             err = "BVH8 is deeper than the traversal stack";
             status = PRT_EINTERNAL;

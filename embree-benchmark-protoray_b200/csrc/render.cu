@@ -51,7 +51,10 @@ __device__ __forceinline__ int warp_append(bool pred, int* counter)
 
 // Lanes refill once at least this many of a warp's 32 lanes are idle
 // (persistent threads with dynamic ray fetch, Aila & Laine, HPG 2009).
-constexpr int kRefillMin = 12;
+#ifndef PRT_REFILL_MIN
+#define PRT_REFILL_MIN 12
+#endif
+constexpr int kRefillMin = PRT_REFILL_MIN;
 
 // Minimum resident 128-thread blocks per SM requested from the compiler for
 // the bounce kernel (8 caps it at 64 registers per thread).

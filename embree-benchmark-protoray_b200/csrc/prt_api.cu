@@ -24,6 +24,9 @@ namespace prt_b200 {
 int replay_max_depth();
 }
 
+constexpr int kMaxChains = 4;
+constexpr int kCounterStride = 64 + 2;   // counters per chain: one per bounce depth (<= 64) + 2
+
 struct prt_ctx
 {
     int device = 0;
@@ -54,12 +57,16 @@ struct prt_ctx
     // render state
     int* dPass = nullptr;                 // device pass counter
     unsigned long long* dRays = nullptr;  // rays of the current call
-    int* dCounts = nullptr;               // [kMaxDepthCap + 2]
-    int* dFetch = nullptr;                // [kMaxDepthCap + 2]
-    PathRec* q[2] = {nullptr, nullptr};
-    float* thr[2] = {nullptr, nullptr};
+    int* dCounts = nullptr;               // [kMaxChains][kMaxDepthCap + 2]
+    int* dFetch = nullptr;                // [kMaxChains][kMaxDepthCap + 2]
+    PathRec* q[kMaxChains][2] = {};       // ping-pong path queues of each concurrent wave chain
+    float* thr[kMaxChains][2] = {};
     long long queueCap = 0;
+    int queueChains = 0;
     bool queueThr = false;
+    cudaStream_t side[kMaxChains] = {};   // streams of the concurrent wave chains (captured into graphs)
+    cudaEvent_t forkEv = nullptr;
+    cudaEvent_t joinEv[kMaxChains] = {};
 
     // query scratch
     RayRec* dRay = nullptr;
@@ -87,7 +94,7 @@ struct prt_ctx
 
 namespace {
 
-constexpr int kMaxDepthCap = 64;
+constexpr int kMaxDepthCap = kCounterStride - 2;
 
 int fail(prt_ctx* c, int status, const std::string& msg)
 {
@@ -162,25 +169,32 @@ __global__ void k_check_indices(const int* idx, long long n3, int nv, int* bad)
     }
 }
 
-int ensure_queues(prt_ctx* ctx, long long paths, bool withThr)
+int ensure_queues(prt_ctx* ctx, long long paths, bool withThr, int chains = 1)
 {
-    if (paths <= ctx->queueCap && (!withThr || ctx->queueThr)) return PRT_OK;
-    for (int i = 0; i < 2; ++i)
-    {
-        cudaFree(ctx->q[i]);
-        cudaFree(ctx->thr[i]);
-        ctx->q[i] = nullptr;
-        ctx->thr[i] = nullptr;
-    }
+    if (paths <= ctx->queueCap && chains <= ctx->queueChains && (!withThr || ctx->queueThr)) return PRT_OK;
+    for (int c = 0; c < kMaxChains; ++c)
+        for (int i = 0; i < 2; ++i)
+        {
+            cudaFree(ctx->q[c][i]);
+            cudaFree(ctx->thr[c][i]);
+            ctx->q[c][i] = nullptr;
+            ctx->thr[c][i] = nullptr;
+        }
     clear_graphs(ctx);
     long long cap = std::max(paths, ctx->queueCap);
-    for (int i = 0; i < 2; ++i)
-    {
-        CK(cudaMalloc(&ctx->q[i], sizeof(PathRec) * (size_t)cap));
-        if (withThr || ctx->queueThr) CK(cudaMalloc(&ctx->thr[i], sizeof(float) * (size_t)cap));
-    }
+    int nch = std::max(chains, ctx->queueChains);
+    bool thr = withThr || ctx->queueThr;
+    ctx->queueCap = 0;
+    ctx->queueChains = 0;
+    for (int c = 0; c < nch; ++c)
+        for (int i = 0; i < 2; ++i)
+        {
+            CK(cudaMalloc(&ctx->q[c][i], sizeof(PathRec) * (size_t)cap));
+            if (thr) CK(cudaMalloc(&ctx->thr[c][i], sizeof(float) * (size_t)cap));
+        }
     ctx->queueCap = cap;
-    ctx->queueThr = withThr || ctx->queueThr;
+    ctx->queueChains = nch;
+    ctx->queueThr = thr;
     return PRT_OK;
 }
 
@@ -202,6 +216,8 @@ float const_throughput(int depth)
     return t;
 }
 
+int chains_for(const prt_ctx* ctx) { return std::max(1, std::min(kMaxChains, ctx->cfg.chains)); }
+
 int passes_per_wave(const prt_ctx* ctx, int spp)
 {
     const long long perPass = (long long)((ctx->W + 7) / 8) * ((ctx->H + 7) / 8) * 64;
@@ -218,40 +234,59 @@ int record_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, int& laun
     const long long perPass = (long long)tilesX * tilesY * 64;
     const int passesPerWave = passes_per_wave(ctx, spp);
     const bool albedo = ctx->dAlbedo != nullptr;
-    if (ctx->queueCap < (long long)passesPerWave * perPass || (albedo && !ctx->queueThr))
+    const int waves = (spp + passesPerWave - 1) / passesPerWave;
+    const int chains = std::max(1, std::min(chains_for(ctx), waves));
+    if (ctx->queueCap < (long long)passesPerWave * perPass || ctx->queueChains < chains || (albedo && !ctx->queueThr))
         return fail(ctx, PRT_EINTERNAL, "path queues too small");
 
     launches = 0;
     if (!accumulate) CK(cudaMemsetAsync(ctx->dAccum, 0, sizeof(float4) * (size_t)W * H, ctx->stream));
     CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+    // waves are dealt round-robin to `chains` streams, so the tail of one
+    // wave's bounce kernel overlaps the work of another wave
+    if (chains > 1)
+    {
+        CK(cudaEventRecord(ctx->forkEv, ctx->stream));
+        for (int c = 0; c < chains; ++c) CK(cudaStreamWaitEvent(ctx->side[c], ctx->forkEv, 0));
+    }
     WaveArgs a;
     a.scene = scene_dev(ctx);
     a.cam = camera_dev(ctx->cam, W, H);
     a.accum = ctx->dAccum;
-    a.counts = ctx->dCounts;
-    a.fetch = ctx->dFetch;
     a.rays = ctx->dRays;
     a.passBase = ctx->dPass;
     a.tilesX = tilesX;
     a.tilesY = tilesY;
     a.maxDepth = maxDepth;
     a.sky = ctx->sky;
-    for (int p0 = 0; p0 < spp; p0 += passesPerWave)
+    for (int w = 0; w < waves; ++w)
     {
-        a.passOffset = p0;
-        a.passes = std::min(passesPerWave, spp - p0);
-        CK(cudaMemsetAsync(ctx->dCounts, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
-        CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+        const int c = w % chains;
+        cudaStream_t s = chains > 1 ? ctx->side[c] : ctx->stream;
+        int* counts = ctx->dCounts + c * kCounterStride;
+        int* fetch = ctx->dFetch + c * kCounterStride;
+        a.counts = counts;
+        a.fetch = fetch;
+        a.passOffset = w * passesPerWave;
+        a.passes = std::min(passesPerWave, spp - w * passesPerWave);
+        CK(cudaMemsetAsync(counts, 0, sizeof(int) * kCounterStride, s));
+        CK(cudaMemsetAsync(fetch, 0, sizeof(int) * kCounterStride, s));
         for (int d = 0; d <= maxDepth; ++d)
         {
-            a.qin = d == 0 ? nullptr : ctx->q[(d - 1) & 1];
-            a.qout = ctx->q[d & 1];
-            a.thrIn = albedo && d > 0 ? ctx->thr[(d - 1) & 1] : nullptr;
-            a.thrOut = albedo ? ctx->thr[d & 1] : nullptr;
+            a.qin = d == 0 ? nullptr : ctx->q[c][(d - 1) & 1];
+            a.qout = ctx->q[c][d & 1];
+            a.thrIn = albedo && d > 0 ? ctx->thr[c][(d - 1) & 1] : nullptr;
+            a.thrOut = albedo ? ctx->thr[c][d & 1] : nullptr;
             a.thrConst = const_throughput(d);
-            launches += launch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
+            launches += launch_bounce(a, d, ctx->cfg, ctx->numSMs, s);
         }
     }
+    if (chains > 1)
+        for (int c = 0; c < chains; ++c)
+        {
+            CK(cudaEventRecord(ctx->joinEv[c], ctx->side[c]));
+            CK(cudaStreamWaitEvent(ctx->stream, ctx->joinEv[c], 0));
+        }
     launches += launch_advance_pass(ctx->dPass, spp, ctx->stream);
     CK(cudaGetLastError());
     return PRT_OK;
@@ -393,11 +428,17 @@ prt_ctx::~prt_ctx()
     cudaFree(dRays);
     cudaFree(dCounts);
     cudaFree(dFetch);
-    for (int i = 0; i < 2; ++i)
+    for (int c = 0; c < kMaxChains; ++c)
     {
-        cudaFree(q[i]);
-        cudaFree(thr[i]);
+        for (int i = 0; i < 2; ++i)
+        {
+            cudaFree(q[c][i]);
+            cudaFree(thr[c][i]);
+        }
+        if (side[c]) cudaStreamDestroy(side[c]);
+        if (joinEv[c]) cudaEventDestroy(joinEv[c]);
     }
+    if (forkEv) cudaEventDestroy(forkEv);
     cudaFree(dRay);
     cudaFree(dHit);
     cudaFree(dPNg);
@@ -431,8 +472,14 @@ int prt_create(int device, prt_ctx** out)
     CK(cudaMalloc(&ctx->dPass, sizeof(int)));
     CK(cudaMemset(ctx->dPass, 0, sizeof(int)));
     CK(cudaMalloc(&ctx->dRays, sizeof(unsigned long long)));
-    CK(cudaMalloc(&ctx->dCounts, sizeof(int) * (kMaxDepthCap + 2)));
-    CK(cudaMalloc(&ctx->dFetch, sizeof(int) * (kMaxDepthCap + 2)));
+    CK(cudaMalloc(&ctx->dCounts, sizeof(int) * kCounterStride * kMaxChains));
+    CK(cudaMalloc(&ctx->dFetch, sizeof(int) * kCounterStride * kMaxChains));
+    CK(cudaEventCreateWithFlags(&ctx->forkEv, cudaEventDisableTiming));
+    for (int c = 0; c < kMaxChains; ++c)
+    {
+        CK(cudaStreamCreateWithFlags(&ctx->side[c], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->joinEv[c], cudaEventDisableTiming));
+    }
     CK(cudaMalloc(&ctx->dRay, sizeof(RayRec)));
     CK(cudaMalloc(&ctx->dHit, sizeof(HitRec)));
     CK(cudaMalloc(&ctx->dPNg, sizeof(float) * 6));
@@ -724,7 +771,10 @@ int prt_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, prt_render_s
     if (spp > 0)
     {
         const long long perPass = (long long)((ctx->W + 7) / 8) * ((ctx->H + 7) / 8) * 64;
-        st = ensure_queues(ctx, (long long)passes_per_wave(ctx, spp) * perPass, ctx->dAlbedo != nullptr);
+        const int ppw = passes_per_wave(ctx, spp);
+        const int waves = (spp + ppw - 1) / ppw;
+        st = ensure_queues(ctx, (long long)ppw * perPass, ctx->dAlbedo != nullptr,
+                           std::max(1, std::min(chains_for(ctx), waves)));
         if (st != PRT_OK) return st;
     }
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -789,10 +839,10 @@ int prt_render_profile(prt_ctx* ctx, int spp, int maxDepth, double* msPerDepth, 
         CK(cudaEventRecord(ev[0], ctx->stream));
         for (int d = 0; d <= maxDepth; ++d)
         {
-            a.qin = d == 0 ? nullptr : ctx->q[(d - 1) & 1];
-            a.qout = ctx->q[d & 1];
-            a.thrIn = albedo && d > 0 ? ctx->thr[(d - 1) & 1] : nullptr;
-            a.thrOut = albedo ? ctx->thr[d & 1] : nullptr;
+            a.qin = d == 0 ? nullptr : ctx->q[0][(d - 1) & 1];
+            a.qout = ctx->q[0][d & 1];
+            a.thrIn = albedo && d > 0 ? ctx->thr[0][(d - 1) & 1] : nullptr;
+            a.thrOut = albedo ? ctx->thr[0][d & 1] : nullptr;
             a.thrConst = const_throughput(d);
             ctx->launches += launch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
             CK(cudaEventRecord(ev[(size_t)d + 1], ctx->stream));
@@ -1013,8 +1063,8 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
             CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
             for (int d = 0; d <= maxDepth; ++d)
             {
-                a.qin = d == 0 ? nullptr : ctx->q[(d - 1) & 1];
-                a.qout = ctx->q[d & 1];
+                a.qin = d == 0 ? nullptr : ctx->q[0][(d - 1) & 1];
+                a.qout = ctx->q[0][d & 1];
                 launches += launch_batch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
             }
         }
@@ -1070,11 +1120,12 @@ int prt_set_tune(prt_ctx* ctx, const prt_tune* t)
 {
     if (!ctx || !t) return PRT_EINVAL;
     if (t->blockSize < 32 || t->blockSize > 128 || (t->blockSize & 31) || t->blocksPerSM < 0 || t->blocksPerSM > 64 ||
-        t->pathsPerWave < 0)
+        t->pathsPerWave < 0 || t->concurrentWaves < 0)
         return fail(ctx, PRT_EINVAL, "invalid launch configuration");
     ctx->cfg.block = t->blockSize;
     ctx->cfg.blocksPerSM = t->blocksPerSM;
     ctx->cfg.pathsPerWave = t->pathsPerWave;
+    ctx->cfg.chains = t->concurrentWaves > 0 ? std::min(t->concurrentWaves, kMaxChains) : ctx->cfg.chains;
     clear_graphs(ctx);
     return PRT_OK;
 }
@@ -1085,6 +1136,7 @@ int prt_get_tune(prt_ctx* ctx, prt_tune* t)
     t->blockSize = ctx->cfg.block;
     t->blocksPerSM = ctx->cfg.blocksPerSM;
     t->pathsPerWave = ctx->cfg.pathsPerWave;
+    t->concurrentWaves = ctx->cfg.chains;
     t->mray = 0;
     return PRT_OK;
 }
@@ -1102,15 +1154,17 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
     const int blocks[] = {64, 128};
     const int perSM[] = {0, 2, 4};
     const long long waves[] = {1, 2, 4};
+    const int chainOpts[] = {1, 2};
     for (int b : blocks)
         for (int s : perSM)
-        {
+            for (int ch : chainOpts)
             for (long long wv : waves)
             {
                 long long ppw = std::max<long long>(perPass * wv, 1 << 16);
                 ctx->cfg.block = b;
                 ctx->cfg.blocksPerSM = s;
                 ctx->cfg.pathsPerWave = (int)std::min<long long>(ppw, 1LL << 30);
+                ctx->cfg.chains = ch;
                 prt_render_stats rs;
                 CK(cudaMemsetAsync(ctx->dPass, 0, sizeof(int), ctx->stream));
                 st = prt_render(ctx, spp, maxDepth, 0, &rs);
@@ -1134,7 +1188,6 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
                 }
                 clear_graphs(ctx);
             }
-        }
     ctx->cfg = bestCfg;
     clear_graphs(ctx);
     st = prt_clear(ctx);
@@ -1144,6 +1197,7 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
         best->blockSize = bestCfg.block;
         best->blocksPerSM = bestCfg.blocksPerSM;
         best->pathsPerWave = bestCfg.pathsPerWave;
+        best->concurrentWaves = bestCfg.chains;
         best->mray = bestMray;
     }
     return PRT_OK;

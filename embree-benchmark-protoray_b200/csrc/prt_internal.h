@@ -95,6 +95,7 @@ struct LaunchCfg
     int block = 128;
     int blocksPerSM = 0;    // 0 = as many as stay resident
     int pathsPerWave = 0;   // 0 = automatic
+    int chains = 2;         // waves in flight at once (concurrent graph branches)
 };
 
 // Kernel launchers (render.cu).  Each returns the number of launches issued.

@@ -76,7 +76,8 @@ class Request(C.Structure):
 
 
 class Tune(C.Structure):
-    _fields_ = [("blockSize", C.c_int), ("blocksPerSM", C.c_int), ("pathsPerWave", C.c_int), ("mray", C.c_double)]
+    _fields_ = [("blockSize", C.c_int), ("blocksPerSM", C.c_int), ("pathsPerWave", C.c_int),
+                ("concurrentWaves", C.c_int), ("mray", C.c_double)]
 
 
 _lib = None
@@ -290,10 +291,11 @@ class Context:
     def autotune(self, spp: int, max_depth: int) -> Dict[str, float]:
         t = Tune()
         self._check(self.L.prt_autotune(self.h, spp, max_depth, C.byref(t)), "prt_autotune")
-        return {"blockSize": t.blockSize, "blocksPerSM": t.blocksPerSM, "pathsPerWave": t.pathsPerWave, "mray": t.mray}
+        return {"blockSize": t.blockSize, "blocksPerSM": t.blocksPerSM, "pathsPerWave": t.pathsPerWave,
+                "concurrentWaves": t.concurrentWaves, "mray": t.mray}
 
-    def set_tune(self, block: int, per_sm: int, paths_per_wave: int):
-        t = Tune(block, per_sm, paths_per_wave, 0.0)
+    def set_tune(self, block: int, per_sm: int, paths_per_wave: int, concurrent_waves: int = 0):
+        t = Tune(block, per_sm, paths_per_wave, concurrent_waves, 0.0)
         self._check(self.L.prt_set_tune(self.h, C.byref(t)), "prt_set_tune")
 
     def render_noalloc(self, cam: Camera, width: int, height: int, pass0: int, spp: int, max_depth: int,

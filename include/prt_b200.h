@@ -108,7 +108,8 @@ typedef struct {
 typedef struct {
     int blockSize;        /* threads per block of the bounce kernel (32..128) */
     int blocksPerSM;      /* resident blocks per SM of the persistent grid */
-    int pathsPerWave;     /* queue capacity (paths in flight per wave) */
+    int pathsPerWave;     /* queue capacity (paths in flight per wave); 0 = automatic */
+    int concurrentWaves;  /* waves in flight at once, 1..4 (0 keeps the current value) */
     double mray;          /* throughput measured for the winner */
 } prt_tune;
 

@@ -13,7 +13,7 @@
 //   5. bottom-up bounds refit (second child to arrive computes the union)
 //   6. top-down collapse into 8-wide nodes, one tree level per launch:
 //      children are opened greedily by largest surface area while fewer than
-//      8 exist; subtrees of <= 3 triangles become leaves; child slots are
+//      8 exist; subtrees of <= leafMax (1..3) triangles become leaves; child slots are
 //      assigned so that slot s holds the child nearest the origin of rays in
 //      direction octant s; child boxes are quantized to 8 bits per axis.
 #include <algorithm>
@@ -369,6 +369,7 @@ struct CollapseArgs
     int* triCounter;
     int nodeCapacity;
     int* error;
+    int leafMax;   // subtrees of at most this many triangles (1..3) become leaves
 };
 
 __device__ __forceinline__ int ref_count(const CollapseArgs& a, int ref)
@@ -418,7 +419,7 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
             float bestA = -1.f;
             for (int i = 0; i < nc; ++i)
             {
-                if (ch[i] < 0 || ref_count(a, ch[i]) <= 3) continue;
+                if (ch[i] < 0 || ref_count(a, ch[i]) <= a.leafMax) continue;
                 float ar = half_area(ref_box(a, ch[i]));
                 if (ar > bestA) { bestA = ar; best = i; }
             }
@@ -473,7 +474,7 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
     for (int i = 0; i < nc; ++i)
     {
         int cnt = ref_count(a, ch[i]);
-        if (cnt > 3) nInternal++;
+        if (cnt > a.leafMax) nInternal++;
         else nTris += cnt;
     }
     int childBase = nInternal ? atomicAdd(a.nodeCounter, nInternal) : 0;
@@ -522,7 +523,7 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
             qhi[k][s] = (uint8_t)fmax(0.0, fmin(255.0, hi));
         }
         int cnt = ref_count(a, ch[i]);
-        if (cnt > 3)
+        if (cnt > a.leafMax)
         {
             meta[s] = (uint8_t)(0x20 | (24 + s));
             imask |= 1u << s;
@@ -580,7 +581,7 @@ inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
     } while (0)
 
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
-               std::string& err, BuildInfo* info)
+               std::string& err, BuildInfo* info, int leafMax)
 {
     (void)nv;
     int status = PRT_OK;
@@ -672,6 +673,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         a.triCounter = counters + 1;
         a.nodeCapacity = nodeCapacity;
         a.error = counters + 3;
+        a.leafMax = std::max(1, std::min(3, leafMax));
         int workCount = 1;
         while (workCount > 0)
         {

@@ -410,7 +410,8 @@ __device__ __forceinline__ void trav_init(TravState& s, const SceneDev& sc, floa
 #endif
 
 template <bool anyHit>
-__device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, const TravRay& r, float tnear, TravStack& st)
+__device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, const TravRay& r, float tnear, TravStack& st,
+                                          uint32_t* nodeVisits = nullptr, uint32_t* triTests = nullptr)
 {
     uint2 ng = s.ng;
     uint32_t tbits, tbase;
@@ -428,6 +429,7 @@ __device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, cons
 #pragma unroll
         for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
         uint32_t hits = node_hits(r, q, tnear, s.tHit);
+        if (nodeVisits) ++*nodeVisits;
         ng = make_uint2(q[1].x, (hits & 0xff000000u) | (q[0].w >> 24));
         tbits = hits & 0x00ffffffu;
         tbase = q[1].y;
@@ -454,6 +456,7 @@ __device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, cons
         float4 a = __ldg(tp), bq = __ldg(tp + 1), c = __ldg(tp + 2);
         int prim = __float_as_int(a.w);
         float t, u, v;
+        if (triTests) ++*triTests;
         if (tri_test(r, f3(a.x, a.y, a.z), f3(bq.x, bq.y, bq.z), f3(c.x, c.y, c.z), tnear, s.tHit, prim, s.primHit,
                      t, u, v))
         {

@@ -39,7 +39,7 @@ struct BuildInfo
 };
 
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
-               std::string& err, BuildInfo* info);
+               std::string& err, BuildInfo* info, int leafMax);
 
 // Arguments of one wave of the wavefront renderer.
 struct WaveArgs

@@ -13,6 +13,17 @@
 
 namespace prt_b200 {
 
+#ifndef PRT_COUNTERS
+#define PRT_COUNTERS 0
+#endif
+
+// Traversal counters of the bounce kernel, compiled in with -DPRT_COUNTERS=1
+// (the reference's RayStats nodeCount/primCount, core/ray_stats.h:23-28):
+//   [0] node visits  [1] triangle tests  [2] rays  [3] warp traversal steps
+//   [4] running lanes summed over steps  [5] warp triangle-loop iterations
+//   (max over the running lanes of a step, summed)
+__device__ unsigned long long g_counters[8];
+
 namespace {
 
 __device__ __forceinline__ void morton8x8(int m, int& x, int& y)
@@ -102,6 +113,8 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
 
     bool has = false;         // this lane holds a ray
     bool exhausted = false;   // warp-uniform: every queue entry has been claimed
+    uint32_t cNodes = 0, cTris = 0, cRays = 0;                          // per lane (PRT_COUNTERS)
+    unsigned long long cSteps = 0, cLaneSteps = 0, cTriIters = 0;       // per warp (PRT_COUNTERS)
     int pixel = 0;
     uint32_t rng = 0;
     float thr = 0.f;
@@ -170,7 +183,20 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
         // --- traverse until the warp has enough idle lanes ------------------
         for (;;)
         {
-            if (has && !ts.done) trav_step<false>(ts, a.scene, r, 0.0f, st);
+            if (PRT_COUNTERS)
+            {
+                unsigned run0 = __ballot_sync(FULL, has && !ts.done);
+                uint32_t tris = 0;
+                if (has && !ts.done) trav_step<false>(ts, a.scene, r, 0.0f, st, &cNodes, &tris);
+                cTris += tris;
+                cLaneSteps += __popc(run0);
+                cSteps += 1;
+                cTriIters += __reduce_max_sync(FULL, tris);
+            }
+            else if (has && !ts.done)
+            {
+                trav_step<false>(ts, a.scene, r, 0.0f, st);
+            }
             unsigned running = __ballot_sync(FULL, has && !ts.done);
             if (running == 0) break;
             if (!exhausted && 32 - __popc(running) >= kRefillMin) break;
@@ -205,7 +231,31 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
         {
             red_add_v4(a.accum + pixel, contrib, contrib, contrib, 1.0f);
         }
-        if (fin) has = false;
+        if (fin)
+        {
+            has = false;
+            ++cRays;
+        }
+    }
+    if (PRT_COUNTERS)
+    {
+        unsigned long long n = cNodes, t = cTris, ry = cRays;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            n += __shfl_down_sync(FULL, n, off);
+            t += __shfl_down_sync(FULL, t, off);
+            ry += __shfl_down_sync(FULL, ry, off);
+        }
+        if (lane == 0)
+        {
+            atomicAdd(&g_counters[0], n);
+            atomicAdd(&g_counters[1], t);
+            atomicAdd(&g_counters[2], ry);
+            atomicAdd(&g_counters[3], cSteps);
+            atomicAdd(&g_counters[4], cLaneSteps);
+            atomicAdd(&g_counters[5], cTriIters);
+        }
     }
 }
 
@@ -665,5 +715,21 @@ int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int p
 }
 
 int replay_max_depth() { return kReplayMaxDepth; }
+
+int read_counters(unsigned long long* out, bool reset, cudaStream_t s)
+{
+    if (!PRT_COUNTERS) return -1;
+    if (cudaMemcpyFromSymbolAsync(out, g_counters, sizeof(g_counters), 0, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return 1;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
+    if (reset)
+    {
+        static const unsigned long long zero[8] = {};
+        if (cudaMemcpyToSymbolAsync(g_counters, zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return 1;
+        if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
+    }
+    return 0;
+}
 
 } // namespace prt_b200

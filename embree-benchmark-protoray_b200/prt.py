@@ -29,11 +29,11 @@ STATUS_NAMES = {0: "PRT_OK", 1: "PRT_EINVAL", 2: "PRT_ENOMEM", 3: "PRT_ECUDA", 4
 EXPORTS = [
     "prt_create", "prt_destroy", "prt_last_error", "prt_get_info",
     "prt_load_mesh", "prt_load_mesh_file", "prt_get_scene_bounds", "prt_set_albedo", "prt_set_sky",
-    "prt_build_accel", "prt_camera_from_view", "prt_set_camera",
+    "prt_build_accel", "prt_set_leaf_size", "prt_camera_from_view", "prt_set_camera",
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
-    "prt_render_batch", "prt_read_accel", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
+    "prt_render_batch", "prt_read_accel", "prt_read_counters", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
 ]
 
 
@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
         "prt_set_albedo": (ip, [vp, vp, ip]),
         "prt_set_sky": (ip, [vp, fp]),
         "prt_build_accel": (ip, [vp, C.POINTER(BuildStats)]),
+        "prt_set_leaf_size": (ip, [vp, ip]),
         "prt_camera_from_view": (ip, [C.POINTER(View), ip, ip, C.POINTER(Camera)]),
         "prt_set_camera": (ip, [vp, C.POINTER(Camera)]),
         "prt_init_frame": (ip, [vp, ip, ip]),
@@ -120,6 +121,7 @@ def lib() -> C.CDLL:
         "prt_render_replay": (ip, [vp, ip, ip, ip, C.POINTER(RenderStats)]),
         "prt_render_batch": (ip, [vp, C.POINTER(Request), ip, C.POINTER(RenderStats)]),
         "prt_read_accel": (ip, [vp, vp, ip, vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "prt_read_counters": (ip, [vp, vp, ip, ip]),
         "prt_autotune": (ip, [vp, ip, ip, C.POINTER(Tune)]),
         "prt_set_tune": (ip, [vp, C.POINTER(Tune)]),
         "prt_get_tune": (ip, [vp, C.POINTER(Tune)]),
@@ -211,6 +213,9 @@ class Context:
 
     def set_sky(self, sky: float):
         self._check(self.L.prt_set_sky(self.h, sky), "prt_set_sky")
+
+    def set_leaf_size(self, n: int):
+        self._check(self.L.prt_set_leaf_size(self.h, n), "prt_set_leaf_size")
 
     def build(self) -> Dict[str, float]:
         s = BuildStats()
@@ -316,6 +321,13 @@ class Context:
         self._check(self.L.prt_read_accel(self.h, nodes.ctypes.data, len(nodes), tris.ctypes.data, len(tris),
                                           C.byref(n), C.byref(t)), "prt_read_accel")
         return nodes[: n.value], tris[: t.value]
+
+    def read_counters(self, reset: bool = True):
+        """Traversal counters (builds with -DPRT_COUNTERS=1), see include/prt_b200.h."""
+        out = np.zeros(6, np.int64)
+        self._check(self.L.prt_read_counters(self.h, out.ctypes.data, 6, int(reset)), "prt_read_counters")
+        keys = ["nodes", "tris", "rays", "steps", "lane_steps", "tri_iters"]
+        return dict(zip(keys, out.tolist()))
 
     def launch_count(self) -> int:
         return int(self.L.prt_launch_count(self.h))

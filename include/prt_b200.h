@@ -135,6 +135,8 @@ int prt_set_sky(prt_ctx* ctx, float sky);
 
 /* --- acceleration structure (OptixIntersectorStreamCuda ctor, accel/optix/optix_intersector_stream_cuda.cpp:23-75) --- */
 int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats);
+/* Largest leaf of the 8-wide tree, 1..3 triangles, for the next build. */
+int prt_set_leaf_size(prt_ctx* ctx, int maxTrianglesPerLeaf);
 
 /* --- camera (DeviceCuda::initCamera, render/device_cuda.cpp:175-200) --- */
 /* Builds the camera of a view for an image of width x height, as the
@@ -202,6 +204,13 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
  * structural tests. */
 int prt_read_accel(prt_ctx* ctx, void* nodes, int nodeCapacity, void* tris, int triCapacity, int* nodeCount,
                    int* triCount);
+
+/* Traversal counters of the bounce kernel since the last reset, in a build
+ * compiled with -DPRT_COUNTERS=1 (the reference's RayStats nodeCount and
+ * primCount, core/ray_stats.h:23-28): out[0] node visits, [1] triangle tests,
+ * [2] rays, [3] warp traversal steps, [4] running lanes summed over steps,
+ * [5] warp triangle-loop iterations.  n >= 6.  Other builds return PRT_ESTATE. */
+int prt_read_counters(prt_ctx* ctx, long long* out, int n, int reset);
 
 /* --- launch configuration --- */
 /* Times candidate bounce-kernel configurations on the current scene/frame

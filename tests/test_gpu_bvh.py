@@ -25,8 +25,9 @@ def _decode(nodes):
     return origin, scale, imask, child, tbase, meta, qlo, qhi
 
 
-@pytest.mark.parametrize("scene", ["small", "batch3", "one", "two"])
-def test_bvh_structure(scene, small):
+@pytest.mark.parametrize("scene,leaf", [("small", 1), ("small", 3), ("batch3", 1), ("batch3", 2), ("one", 1),
+                                        ("two", 1), ("two", 3)])
+def test_bvh_structure(scene, leaf, small):
     import prt
     import scenes
     if scene == "small":
@@ -43,6 +44,7 @@ def test_bvh_structure(scene, small):
         idx = np.array([[0, 1, 2], [0, 1, 3]], np.int32)
     c = prt.Context(0)
     c.load_mesh(idx, pos)
+    c.set_leaf_size(leaf)
     st = c.build()
     nodes, tris = c.read_accel()
     assert 2 * st["levels"] <= 64
@@ -81,7 +83,7 @@ def test_bvh_structure(scene, small):
                 assert np.all(clo.min(axis=1) >= lo - eps) and np.all(chi.max(axis=1) <= hi + eps + 255 * scale[ci])
             else:
                 cnt = bin(m >> 5).count("1")
-                assert (m >> 5) == (1 << cnt) - 1 and 1 <= cnt <= 3
+                assert (m >> 5) == (1 << cnt) - 1 and 1 <= cnt <= leaf
                 off = m & 0x1F
                 for k in range(cnt):
                     t = tbase[i] + off + k

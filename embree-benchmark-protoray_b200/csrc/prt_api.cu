@@ -364,64 +364,222 @@ int check_ready(prt_ctx* ctx, bool needFrame)
     return PRT_OK;
 }
 
-// --- .mesh blob reader (geometry/triangle_mesh.cpp:305-320, sys/blob.h:26-38) ---
-struct MeshFile
+__global__ void k_deinterleave(const float* __restrict__ attrs, int stride, int nv, float* __restrict__ pos)
 {
-    std::vector<int> idx;
-    std::vector<float> pos;
-    float lo[3], hi[3];
-};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3LL * nv;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        long long v = i / 3;
+        int k = (int)(i - 3 * v);
+        pos[i] = attrs[v * stride + k];
+    }
+}
 
-int read_mesh_file(prt_ctx* ctx, const char* path, MeshFile& m)
+__global__ void k_bounds_partial(const float* __restrict__ pos, int nv, float* __restrict__ partial)
 {
-    std::ifstream f(path, std::ios::binary);
-    if (!f) return fail(ctx, PRT_EIO, std::string("cannot open ") + path);
-    f.seekg(0, std::ios::end);
-    long long size = f.tellg();
-    f.seekg(0);
-    std::vector<char> data((size_t)std::max<long long>(size, 0));
-    if (size > 0) f.read(data.data(), size);
-    if (!f) return fail(ctx, PRT_EIO, std::string("read error: ") + path);
-    size_t off = 0;
-    auto take = [&](void* dst, size_t n) {
-        if (off + n > data.size()) return false;
-        std::memcpy(dst, data.data() + off, n);
-        off += n;
-        return true;
-    };
-    int id = 0;
-    if (!take(&id, 4)) return fail(ctx, PRT_EIO, "unexpected end of stream");
-    if (id != 0x04df8666) return fail(ctx, PRT_EIO, std::string("file has wrong blob ID: ") + path);
-    float b[6];
-    int tri = 0, vert = 0;
-    unsigned char hasN = 0, hasT = 0;
-    if (!take(b, 24) || !take(&tri, 4) || !take(&vert, 4) || !take(&hasN, 1) || !take(&hasT, 1))
-        return fail(ctx, PRT_EIO, "unexpected end of stream");
-    if (tri < 0 || vert < 0) return fail(ctx, PRT_EIO, "negative element count");
-    int stride = 3 + (hasN ? 3 : 0) + (hasT ? 2 : 0);
-    m.idx.resize(3 * (size_t)tri);
-    std::vector<int> mat((size_t)tri);
-    std::vector<float> attrs((size_t)vert * stride);
-    if (!take(m.idx.data(), 12 * (size_t)tri) || !take(mat.data(), 4 * (size_t)tri) ||
-        !take(attrs.data(), 4 * attrs.size()))
-        return fail(ctx, PRT_EIO, "unexpected end of stream");
-    int nnames = 0;
-    if (!take(&nnames, 4) || nnames < 0) return fail(ctx, PRT_EIO, "unexpected end of stream");
-    for (int i = 0; i < nnames; ++i)
-    {
-        int len = 0;
-        if (!take(&len, 4) || len < 0 || off + (size_t)len > data.size())
-            return fail(ctx, PRT_EIO, "unexpected end of stream");
-        off += (size_t)len;
-    }
-    m.pos.resize(3 * (size_t)vert);
-    for (int v = 0; v < vert; ++v)
-        for (int k = 0; k < 3; ++k) m.pos[3 * (size_t)v + k] = attrs[(size_t)v * stride + k];
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        for (int k = 0; k < 3; ++k)
+        {
+            float x = pos[3 * (size_t)v + k];
+            lo[k] = fminf(lo[k], x);
+            hi[k] = fmaxf(hi[k], x);
+        }
     for (int k = 0; k < 3; ++k)
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            lo[k] = fminf(lo[k], __shfl_down_sync(0xffffffffu, lo[k], off));
+            hi[k] = fmaxf(hi[k], __shfl_down_sync(0xffffffffu, hi[k], off));
+        }
+    if ((threadIdx.x & 31) == 0)
     {
-        m.lo[k] = b[k];
-        m.hi[k] = b[3 + k];
+        int w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+        for (int k = 0; k < 3; ++k)
+        {
+            partial[6 * w + k] = lo[k];
+            partial[6 * w + 3 + k] = hi[k];
+        }
     }
+}
+
+// Takes ownership of device arrays dIdx (3*nt ints) and dPos (3*nv floats):
+// checks every index, then makes them the context's mesh.  lo/hi: the stored
+// scene box, or nullptr to compute it on the device.
+int install_mesh(prt_ctx* ctx, int* dIdx, float* dPos, int nt, int nv, const float* lo, const float* hi)
+{
+    auto drop = [&]() {
+        cudaFree(dIdx);
+        cudaFree(dPos);
+    };
+    int* dBad = nullptr;
+    float* dPart = nullptr;
+    const int blocks = 128, threads = 256, warps = blocks * threads / 32;
+    cudaError_t e = cudaMalloc(&dBad, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&dPart, sizeof(float) * 6 * warps);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dBad, 0, sizeof(int), ctx->stream);
+    if (e == cudaSuccess && nt)
+    {
+        // every index must name a vertex: the kernels gather positions unchecked
+        k_check_indices<<<256, 256, 0, ctx->stream>>>(dIdx, 3LL * nt, nv, dBad);
+        ctx->launches++;
+    }
+    if (e == cudaSuccess && nv && !lo)
+    {
+        k_bounds_partial<<<blocks, threads, 0, ctx->stream>>>(dPos, nv, dPart);
+        ctx->launches++;
+    }
+    int bad = 0;
+    std::vector<float> part((size_t)6 * warps);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, dBad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && nv && !lo)
+        e = cudaMemcpyAsync(part.data(), dPart, sizeof(float) * part.size(), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(dBad);
+    cudaFree(dPart);
+    if (e != cudaSuccess)
+    {
+        drop();
+        return fail(ctx, e == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA, cudaGetErrorString(e));
+    }
+    if (bad)
+    {
+        drop();
+        return fail(ctx, PRT_EINVAL, "triangle index out of range");
+    }
+    float blo[3] = {0, 0, 0}, bhi[3] = {0, 0, 0};
+    if (lo)
+    {
+        std::memcpy(blo, lo, sizeof(blo));
+        std::memcpy(bhi, hi, sizeof(bhi));
+    }
+    else if (nv)
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            blo[k] = FLT_MAX;
+            bhi[k] = -FLT_MAX;
+        }
+        for (int w = 0; w < warps; ++w)
+            for (int k = 0; k < 3; ++k)
+            {
+                blo[k] = std::min(blo[k], part[6 * (size_t)w + k]);
+                bhi[k] = std::max(bhi[k], part[6 * (size_t)w + 3 + k]);
+            }
+    }
+    clear_graphs(ctx);
+    ctx->bvh.release();
+    ctx->built = false;
+    cudaFree(ctx->dPos);
+    cudaFree(ctx->dIdx);
+    cudaFree(ctx->dAlbedo);
+    ctx->dAlbedo = nullptr;
+    ctx->dPos = dPos;
+    ctx->dIdx = dIdx;
+    ctx->nt = nt;
+    ctx->nv = nv;
+    std::memcpy(ctx->lo, blo, sizeof(blo));
+    std::memcpy(ctx->hi, bhi, sizeof(bhi));
+    ctx->haveMesh = true;
+    return PRT_OK;
+}
+
+// .mesh blob loader (geometry/triangle_mesh.cpp:305-320, sys/blob.h:26-38).
+// The layout is validated against the file length first; the index and
+// vertex-attribute blocks are then read straight into pinned host memory,
+// copied to the device asynchronously, and the interleaved attributes
+// (position [+ normal] [+ uv], geometry/triangle_mesh.cpp:29-56) are
+// de-interleaved on the GPU.
+int load_mesh_file(prt_ctx* ctx, const char* path, float outLo[3], float outHi[3])
+{
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, PRT_EIO, std::string("cannot open ") + path);
+    struct Closer
+    {
+        FILE* f;
+        ~Closer() { std::fclose(f); }
+    } closer{f};
+    std::fseek(f, 0, SEEK_END);
+    const long long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    unsigned char head[38];
+    if (size < 38 || std::fread(head, 1, 38, f) != 38) return fail(ctx, PRT_EIO, "unexpected end of stream");
+    int id, tri, vert;
+    float b[6];
+    std::memcpy(&id, head, 4);
+    if (id != 0x04df8666) return fail(ctx, PRT_EIO, std::string("file has wrong blob ID: ") + path);
+    std::memcpy(b, head + 4, 24);
+    std::memcpy(&tri, head + 28, 4);
+    std::memcpy(&vert, head + 32, 4);
+    const bool hasN = head[36] != 0, hasT = head[37] != 0;
+    if (tri < 0 || vert < 0) return fail(ctx, PRT_EIO, "negative element count");
+    const int stride = 3 + (hasN ? 3 : 0) + (hasT ? 2 : 0);
+    const size_t idxBytes = 12 * (size_t)tri, matBytes = 4 * (size_t)tri, attrBytes = 4 * (size_t)vert * stride;
+    const long long namesAt = 38 + (long long)(idxBytes + matBytes + attrBytes);
+    if (namesAt + 4 > size) return fail(ctx, PRT_EIO, "unexpected end of stream");
+    // material names: int count + (int length + bytes) each (sys/array.h:357-392)
+    {
+        std::fseek(f, (long)namesAt, SEEK_SET);
+        int n = 0;
+        if (std::fread(&n, 4, 1, f) != 1 || n < 0) return fail(ctx, PRT_EIO, "unexpected end of stream");
+        long long at = namesAt + 4;
+        for (int i = 0; i < n; ++i)
+        {
+            int len = 0;
+            if (std::fread(&len, 4, 1, f) != 1 || len < 0 || at + 4 + len > size)
+                return fail(ctx, PRT_EIO, "unexpected end of stream");
+            at += 4 + len;
+            std::fseek(f, (long)at, SEEK_SET);
+        }
+    }
+    char* pinned = nullptr;
+    int* dIdx = nullptr;
+    float* dPos = nullptr;
+    float* dAttr = nullptr;
+    auto cleanup = [&]() {
+        if (pinned) cudaFreeHost(pinned);
+        if (dAttr && dAttr != dPos) cudaFree(dAttr);
+    };
+    cudaError_t e = cudaHostAlloc(&pinned, std::max<size_t>(idxBytes + attrBytes, 16), cudaHostAllocDefault);
+    if (e != cudaSuccess) return fail(ctx, PRT_ENOMEM, "cannot allocate pinned staging memory");
+    std::fseek(f, 38, SEEK_SET);
+    bool ok = std::fread(pinned, 1, idxBytes, f) == idxBytes;
+    ok = ok && std::fseek(f, (long)(38 + idxBytes + matBytes), SEEK_SET) == 0;
+    ok = ok && std::fread(pinned + idxBytes, 1, attrBytes, f) == attrBytes;
+    if (!ok)
+    {
+        cleanup();
+        return fail(ctx, PRT_EIO, std::string("read error: ") + path);
+    }
+    e = cudaMalloc(&dIdx, std::max<size_t>(idxBytes, 12));
+    if (e == cudaSuccess) e = cudaMalloc(&dPos, sizeof(float) * 3 * (size_t)std::max(vert, 1));
+    if (e == cudaSuccess)
+    {
+        if (stride == 3) dAttr = dPos;
+        else e = cudaMalloc(&dAttr, std::max<size_t>(attrBytes, 4));
+    }
+    if (e == cudaSuccess && idxBytes) e = cudaMemcpyAsync(dIdx, pinned, idxBytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && attrBytes)
+        e = cudaMemcpyAsync(dAttr, pinned + idxBytes, attrBytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && stride != 3 && vert)
+    {
+        k_deinterleave<<<512, 256, 0, ctx->stream>>>(dAttr, stride, vert, dPos);
+        ctx->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cleanup();
+    if (e != cudaSuccess)
+    {
+        cudaFree(dIdx);
+        cudaFree(dPos);
+        return fail(ctx, e == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA, cudaGetErrorString(e));
+    }
+    float lo[3] = {b[0], b[1], b[2]}, hi[3] = {b[3], b[4], b[5]};
+    int st = install_mesh(ctx, dIdx, dPos, tri, vert, lo, hi);
+    if (st != PRT_OK) return st;
+    if (outLo) std::memcpy(outLo, lo, sizeof(lo));
+    if (outHi) std::memcpy(outHi, hi, sizeof(hi));
     return PRT_OK;
 }
 
@@ -523,72 +681,28 @@ int prt_load_mesh(prt_ctx* ctx, const int* indices, int triCount, const float* p
     if (triCount < 0 || vertCount < 0) return fail(ctx, PRT_EINVAL, "negative element count");
     if ((triCount > 0 && !indices) || (vertCount > 0 && !positions)) return fail(ctx, PRT_EINVAL, "null mesh array");
     CK(cudaSetDevice(ctx->device));
-    clear_graphs(ctx);
-    ctx->bvh.release();
-    ctx->built = false;
-    cudaFree(ctx->dPos);
-    cudaFree(ctx->dIdx);
-    cudaFree(ctx->dAlbedo);
-    ctx->dPos = nullptr;
-    ctx->dIdx = nullptr;
-    ctx->dAlbedo = nullptr;
-    ctx->haveMesh = false;
-    CK(cudaMalloc(&ctx->dPos, sizeof(float) * 3 * (size_t)std::max(vertCount, 1)));
-    CK(cudaMalloc(&ctx->dIdx, sizeof(int) * 3 * (size_t)std::max(triCount, 1)));
-    if (vertCount)
-        CK(cudaMemcpyAsync(ctx->dPos, positions, sizeof(float) * 3 * (size_t)vertCount, cudaMemcpyDefault, ctx->stream));
-    if (triCount)
-        CK(cudaMemcpyAsync(ctx->dIdx, indices, sizeof(int) * 3 * (size_t)triCount, cudaMemcpyDefault, ctx->stream));
-    // every index must name a vertex: the kernels gather positions unchecked
-    int* dBad = nullptr;
-    CK(cudaMalloc(&dBad, sizeof(int)));
-    CK(cudaMemsetAsync(dBad, 0, sizeof(int), ctx->stream));
-    if (triCount)
+    int* dIdx = nullptr;
+    float* dPos = nullptr;
+    cudaError_t e = cudaMalloc(&dPos, sizeof(float) * 3 * (size_t)std::max(vertCount, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&dIdx, sizeof(int) * 3 * (size_t)std::max(triCount, 1));
+    if (e == cudaSuccess && vertCount)
+        e = cudaMemcpyAsync(dPos, positions, sizeof(float) * 3 * (size_t)vertCount, cudaMemcpyDefault, ctx->stream);
+    if (e == cudaSuccess && triCount)
+        e = cudaMemcpyAsync(dIdx, indices, sizeof(int) * 3 * (size_t)triCount, cudaMemcpyDefault, ctx->stream);
+    if (e != cudaSuccess)
     {
-        k_check_indices<<<256, 256, 0, ctx->stream>>>(ctx->dIdx, 3LL * triCount, vertCount, dBad);
-        ctx->launches++;
+        cudaFree(dPos);
+        cudaFree(dIdx);
+        return fail(ctx, e == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA, cudaGetErrorString(e));
     }
-    int bad = 0;
-    CK(cudaMemcpyAsync(&bad, dBad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    cudaFree(dBad);
-    if (bad) return fail(ctx, PRT_EINVAL, "triangle index out of range");
-    // bounds (host copy of the positions when they came from the host)
-    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    if (vertCount)
-    {
-        std::vector<float> hp(3 * (size_t)vertCount);
-        CK(cudaMemcpy(hp.data(), ctx->dPos, sizeof(float) * hp.size(), cudaMemcpyDeviceToHost));
-        for (int k = 0; k < 3; ++k) { lo[k] = hp[k]; hi[k] = hp[k]; }
-        for (int v = 1; v < vertCount; ++v)
-            for (int k = 0; k < 3; ++k)
-            {
-                lo[k] = std::min(lo[k], hp[3 * (size_t)v + k]);
-                hi[k] = std::max(hi[k], hp[3 * (size_t)v + k]);
-            }
-    }
-    std::memcpy(ctx->lo, lo, sizeof(lo));
-    std::memcpy(ctx->hi, hi, sizeof(hi));
-    ctx->nt = triCount;
-    ctx->nv = vertCount;
-    ctx->haveMesh = true;
-    return PRT_OK;
+    return install_mesh(ctx, dIdx, dPos, triCount, vertCount, nullptr, nullptr);
 }
 
 int prt_load_mesh_file(prt_ctx* ctx, const char* path, float boundsLo[3], float boundsHi[3])
 {
     if (!ctx || !path) return PRT_EINVAL;
-    MeshFile m;
-    int st = read_mesh_file(ctx, path, m);
-    if (st != PRT_OK) return st;
-    st = prt_load_mesh(ctx, m.idx.data(), (int)(m.idx.size() / 3), m.pos.data(), (int)(m.pos.size() / 3));
-    if (st != PRT_OK) return st;
-    // the stored box is the scene bounds of the reference (TriangleMesh::bounds)
-    std::memcpy(ctx->lo, m.lo, sizeof(m.lo));
-    std::memcpy(ctx->hi, m.hi, sizeof(m.hi));
-    if (boundsLo) std::memcpy(boundsLo, m.lo, sizeof(m.lo));
-    if (boundsHi) std::memcpy(boundsHi, m.hi, sizeof(m.hi));
-    return PRT_OK;
+    CK(cudaSetDevice(ctx->device));
+    return load_mesh_file(ctx, path, boundsLo, boundsHi);
 }
 
 int prt_get_scene_bounds(prt_ctx* ctx, float lo[3], float hi[3])

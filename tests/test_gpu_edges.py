@@ -149,3 +149,33 @@ def test_mesh_file_matches_arrays(small, small_path):
         c.set_view(view, 32, 32)
         c.render(2, 3)
     np.testing.assert_array_equal(a.read_accum(), b.read_accum())
+
+
+def test_mesh_file_with_normals_and_uvs(tmp_path):
+    """Interleaved position/normal/uv attributes (stride 8) are de-interleaved
+    on the GPU (geometry/triangle_mesh.cpp:29-56)."""
+    import prt
+    rng = np.random.default_rng(1)
+    nv, nt = 50, 40
+    pos = rng.uniform(-1, 1, (nv, 3)).astype(np.float32)
+    nrm = rng.normal(size=(nv, 3)).astype(np.float32)
+    uv = rng.uniform(0, 1, (nv, 2)).astype(np.float32)
+    idx = rng.integers(0, nv, (nt, 3)).astype(np.int32)
+    attrs = np.concatenate([pos, nrm, uv], axis=1)
+    path = tmp_path / "nuv.mesh"
+    with open(path, "wb") as f:
+        f.write(struct.pack("<i", 0x04DF8666))
+        f.write(struct.pack("<6f", *pos.min(0), *pos.max(0)))
+        f.write(struct.pack("<ii??", nt, nv, True, True))
+        f.write(idx.tobytes())
+        f.write(np.zeros(nt, np.int32).tobytes())
+        f.write(attrs.tobytes())
+        f.write(struct.pack("<i", 1) + struct.pack("<i", 3) + b"mat")
+    c = prt.Context(0)
+    lo, hi = c.load_mesh_file(str(path))
+    np.testing.assert_array_equal(lo, pos.min(0))
+    c.build()
+    _, tris = c.read_accel()
+    prims = tris[:, 3].view(np.int32)
+    np.testing.assert_array_equal(tris[:, 0:3], pos[idx[prims, 0]])
+    np.testing.assert_array_equal(tris[:, 8:11], pos[idx[prims, 2]])

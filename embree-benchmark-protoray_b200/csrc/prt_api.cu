@@ -73,7 +73,10 @@ struct prt_ctx
     int* dFetch = nullptr;                // [kMaxChains][kMaxDepthCap + 2]
     PathRec* q[kMaxChains][2] = {};       // ping-pong path queues of each concurrent wave chain
     float* thr[kMaxChains][2] = {};
+    float* Lq[kMaxChains][2] = {};        // next-event estimation: gathered radiance per path
     long long queueCap = 0;
+    bool queueL = false;
+    int integrator = PRT_INTEGRATOR_DIFFUSE;
     int queueChains = 0;
     bool queueThr = false;
     cudaStream_t side[kMaxChains] = {};   // streams of the concurrent wave chains (captured into graphs)
@@ -181,21 +184,25 @@ __global__ void k_check_indices(const int* idx, long long n3, int nv, int* bad)
     }
 }
 
-int ensure_queues(prt_ctx* ctx, long long paths, bool withThr, int chains = 1)
+int ensure_queues(prt_ctx* ctx, long long paths, bool withThr, int chains = 1, bool withL = false)
 {
-    if (paths <= ctx->queueCap && chains <= ctx->queueChains && (!withThr || ctx->queueThr)) return PRT_OK;
+    if (paths <= ctx->queueCap && chains <= ctx->queueChains && (!withThr || ctx->queueThr) && (!withL || ctx->queueL))
+        return PRT_OK;
     for (int c = 0; c < kMaxChains; ++c)
         for (int i = 0; i < 2; ++i)
         {
             cudaFree(ctx->q[c][i]);
             cudaFree(ctx->thr[c][i]);
+            cudaFree(ctx->Lq[c][i]);
             ctx->q[c][i] = nullptr;
             ctx->thr[c][i] = nullptr;
+            ctx->Lq[c][i] = nullptr;
         }
     clear_graphs(ctx);
     long long cap = std::max(paths, ctx->queueCap);
     int nch = std::max(chains, ctx->queueChains);
     bool thr = withThr || ctx->queueThr;
+    bool lq = withL || ctx->queueL;
     ctx->queueCap = 0;
     ctx->queueChains = 0;
     for (int c = 0; c < nch; ++c)
@@ -203,10 +210,12 @@ int ensure_queues(prt_ctx* ctx, long long paths, bool withThr, int chains = 1)
         {
             CK(cudaMalloc(&ctx->q[c][i], sizeof(PathRec) * (size_t)cap));
             if (thr) CK(cudaMalloc(&ctx->thr[c][i], sizeof(float) * (size_t)cap));
+            if (lq) CK(cudaMalloc(&ctx->Lq[c][i], sizeof(float) * (size_t)cap));
         }
     ctx->queueCap = cap;
     ctx->queueChains = nch;
     ctx->queueThr = thr;
+    ctx->queueL = lq;
     return PRT_OK;
 }
 
@@ -248,7 +257,9 @@ int record_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, int& laun
     const bool albedo = ctx->dAlbedo != nullptr;
     const int waves = (spp + passesPerWave - 1) / passesPerWave;
     const int chains = std::max(1, std::min(chains_for(ctx), waves));
-    if (ctx->queueCap < (long long)passesPerWave * perPass || ctx->queueChains < chains || (albedo && !ctx->queueThr))
+    const bool nee = ctx->integrator == PRT_INTEGRATOR_DIFFUSE2;
+    if (ctx->queueCap < (long long)passesPerWave * perPass || ctx->queueChains < chains ||
+        (albedo && !ctx->queueThr) || (nee && !ctx->queueL))
         return fail(ctx, PRT_EINTERNAL, "path queues too small");
 
     launches = 0;
@@ -289,6 +300,8 @@ int record_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, int& laun
             a.qout = ctx->q[c][d & 1];
             a.thrIn = albedo && d > 0 ? ctx->thr[c][(d - 1) & 1] : nullptr;
             a.thrOut = albedo ? ctx->thr[c][d & 1] : nullptr;
+            a.Lin = nee && d > 0 ? ctx->Lq[c][(d - 1) & 1] : nullptr;
+            a.Lout = nee ? ctx->Lq[c][d & 1] : nullptr;
             a.thrConst = const_throughput(d);
             launches += launch_bounce(a, d, ctx->cfg, ctx->numSMs, s);
         }
@@ -604,6 +617,7 @@ prt_ctx::~prt_ctx()
         {
             cudaFree(q[c][i]);
             cudaFree(thr[c][i]);
+            cudaFree(Lq[c][i]);
         }
         if (side[c]) cudaStreamDestroy(side[c]);
         if (joinEv[c]) cudaEventDestroy(joinEv[c]);
@@ -731,6 +745,16 @@ int prt_set_albedo(prt_ctx* ctx, const float* albedo, int triCount)
     if (ctx->nt)
         CK(cudaMemcpyAsync(ctx->dAlbedo, albedo, sizeof(float) * (size_t)ctx->nt, cudaMemcpyDefault, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_set_integrator(prt_ctx* ctx, int integrator)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (integrator != PRT_INTEGRATOR_DIFFUSE && integrator != PRT_INTEGRATOR_DIFFUSE2)
+        return fail(ctx, PRT_EINVAL, "unknown integrator");
+    if (integrator != ctx->integrator) clear_graphs(ctx);
+    ctx->integrator = integrator;
     return PRT_OK;
 }
 
@@ -908,14 +932,15 @@ int prt_render(prt_ctx* ctx, int spp, int maxDepth, int accumulate, prt_render_s
         const int ppw = passes_per_wave(ctx, spp);
         const int waves = (spp + ppw - 1) / ppw;
         st = ensure_queues(ctx, (long long)ppw * perPass, ctx->dAlbedo != nullptr,
-                           std::max(1, std::min(chains_for(ctx), waves)));
+                           std::max(1, std::min(chains_for(ctx), waves)),
+                           ctx->integrator == PRT_INTEGRATOR_DIFFUSE2);
         if (st != PRT_OK) return st;
     }
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (spp > 0)
     {
         std::ostringstream key;
-        key << "render:" << spp << ":" << maxDepth << ":" << accumulate << ":" << ctx->cfg.block << ":"
+        key << "render:" << ctx->integrator << ":" << spp << ":" << maxDepth << ":" << accumulate << ":" << ctx->cfg.block << ":"
             << ctx->cfg.blocksPerSM << ":" << ctx->cfg.pathsPerWave;
         int launches = 0;
         st = run_graph(ctx, key.str(), [&](int& l) { return record_render(ctx, spp, maxDepth, accumulate, l); },
@@ -942,7 +967,8 @@ int prt_render_profile(prt_ctx* ctx, int spp, int maxDepth, double* msPerDepth, 
     const long long perPass = (long long)tilesX * tilesY * 64;
     const int ppw = passes_per_wave(ctx, spp);
     const bool albedo = ctx->dAlbedo != nullptr;
-    st = ensure_queues(ctx, (long long)ppw * perPass, albedo);
+    const bool nee = ctx->integrator == PRT_INTEGRATOR_DIFFUSE2;
+    st = ensure_queues(ctx, (long long)ppw * perPass, albedo, 1, nee);
     if (st != PRT_OK) return st;
     for (int d = 0; d <= maxDepth; ++d)
     {
@@ -977,6 +1003,8 @@ int prt_render_profile(prt_ctx* ctx, int spp, int maxDepth, double* msPerDepth, 
             a.qout = ctx->q[0][d & 1];
             a.thrIn = albedo && d > 0 ? ctx->thr[0][(d - 1) & 1] : nullptr;
             a.thrOut = albedo ? ctx->thr[0][d & 1] : nullptr;
+            a.Lin = nee && d > 0 ? ctx->Lq[0][(d - 1) & 1] : nullptr;
+            a.Lout = nee ? ctx->Lq[0][d & 1] : nullptr;
             a.thrConst = const_throughput(d);
             ctx->launches += launch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
             CK(cudaEventRecord(ev[(size_t)d + 1], ctx->stream));

@@ -411,7 +411,8 @@ __device__ __forceinline__ void trav_init(TravState& s, const SceneDev& sc, floa
 
 template <bool anyHit>
 __device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, const TravRay& r, float tnear, TravStack& st,
-                                          uint32_t* nodeVisits = nullptr, uint32_t* triTests = nullptr)
+                                          uint32_t* nodeVisits = nullptr, uint32_t* triTests = nullptr,
+                                          bool anyHitRt = false)
 {
     uint2 ng = s.ng;
     uint32_t tbits, tbase;
@@ -465,7 +466,7 @@ __device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, cons
             s.uHit = u;
             s.vHit = v;
             s.triHit = ti;
-            if (anyHit)
+            if (anyHit || anyHitRt)
             {
                 s.done = true;
                 return;
@@ -506,12 +507,21 @@ __device__ __forceinline__ int traverse(const SceneDev& sc, const TravRay& r, fl
 // normal flipped against the ray, frame from makeFrame (math/basis3.h:128-137),
 // cosine-weighted direction (sampling/shape_sampler.h:50-74), and the origin
 // offset by eps along the new direction (core/ray.h:47-52).
-__device__ __forceinline__ void diffuse_bounce(const TriRec* tris, int triIdx, float3& org, float3& dir, float t,
-                                               uint32_t& rng)
+// Shading frame of a hit: point p, offset eps, geometric normal N facing the
+// ray, and the tangents U, V of makeFrame.
+struct HitFrame
 {
-    float3 p = madd(org, t, dir);
-    float m = fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z)));
-    float eps = __fmul_rn(fmaxf(t, m), 0x1.fp-18f);
+    float3 p;
+    float eps;
+    float3 U, V, N;
+};
+
+__device__ __forceinline__ HitFrame hit_frame(const TriRec* tris, int triIdx, float3 org, float3 dir, float t)
+{
+    HitFrame h;
+    h.p = madd(org, t, dir);
+    float m = fmaxf(fabsf(h.p.x), fmaxf(fabsf(h.p.y), fabsf(h.p.z)));
+    h.eps = __fmul_rn(fmaxf(t, m), 0x1.fp-18f);
     const float4* tp = reinterpret_cast<const float4*>(tris + triIdx);
     float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
     float3 p0 = f3(a.x, a.y, a.z), p1 = f3(b.x, b.y, b.z), p2 = f3(c.x, c.y, c.z);
@@ -520,9 +530,16 @@ __device__ __forceinline__ void diffuse_bounce(const TriRec* tris, int triIdx, f
     // makeFrame
     float3 U0 = f3(0.0f, Ng.z, -Ng.y);
     float3 U1 = f3(-Ng.z, 0.0f, Ng.x);
-    float3 U = normalize(dot(U0, U0) > dot(U1, U1) ? U0 : U1);
-    float3 V = normalize(cross(Ng, U));
-    // cosine-weighted hemisphere sample
+    h.U = normalize(dot(U0, U0) > dot(U1, U1) ? U0 : U1);
+    h.V = normalize(cross(Ng, h.U));
+    h.N = Ng;
+    return h;
+}
+
+// A cosine-weighted direction about the frame (two RNG draws) and the ray
+// origin offset along it.
+__device__ __forceinline__ void sample_bounce(const HitFrame& h, uint32_t& rng, float3& org, float3& dir)
+{
     float sx = rng_next(rng);
     float sy = rng_next(rng);
     float cosT = __fsqrt_rn(sx);
@@ -530,9 +547,15 @@ __device__ __forceinline__ void diffuse_bounce(const TriRec* tris, int triIdx, f
     float sphi, cphi;
     sincosf(__fmul_rn(2.0f * 3.14159265358979f, sy), &sphi, &cphi);
     float lx = __fmul_rn(cphi, sinT), ly = __fmul_rn(sphi, sinT);
-    float3 nd = add(add(mul(U, lx), mul(V, ly)), mul(Ng, cosT));
-    dir = nd;
-    org = madd(p, eps, nd);
+    dir = add(add(mul(h.U, lx), mul(h.V, ly)), mul(h.N, cosT));
+    org = madd(h.p, h.eps, dir);
+}
+
+__device__ __forceinline__ void diffuse_bounce(const TriRec* tris, int triIdx, float3& org, float3& dir, float t,
+                                               uint32_t& rng)
+{
+    HitFrame h = hit_frame(tris, triIdx, org, dir, t);
+    sample_bounce(h, rng, org, dir);
 }
 
 // Fire-and-forget vector add into the accumulation buffer (sm_90+).

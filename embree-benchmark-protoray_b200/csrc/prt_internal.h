@@ -61,6 +61,8 @@ struct WaveArgs
     int maxDepth;
     float thrConst;            // throughput at this depth when albedo is constant
     float sky;
+    float* Lin = nullptr;      // next-event estimation: radiance gathered so far, per path
+    float* Lout = nullptr;     // (nullptr for the plain diffuse integrator)
 };
 
 // Per-request table entry of the batched renderer.

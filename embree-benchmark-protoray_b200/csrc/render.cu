@@ -259,6 +259,176 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
     }
 }
 
+// Bounce kernel of the next-event-estimation integrator
+// (render/diffuse2_integrator_single.h:41-90, render/diffuse2_renderer_cuda.cu:63-239).
+// A lane takes a path's extension ray; at a hit before maxDepth it samples a
+// shadow direction and an extension direction from the same frame, traces the
+// shadow ray for any occluder in the same lane (+0.5 * throughput * sky if it
+// escapes), then appends the extension ray with its gathered radiance.  An
+// escaping extension ray adds throughput * sky weighted 1 from the camera and
+// 0.5 after a bounce.  Shadow rays are counted as rays.
+template <bool kFirst, bool kAlbedo>
+__global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveArgs a, int depth)
+{
+    extern __shared__ uint2 s_stack[];
+    TravStack st;
+    st.sh = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    st.overflow = false;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned ltMask = (1u << lane) - 1u;
+    const int W = a.cam.width, H = a.cam.height;
+    const int perPass = a.tilesX * a.tilesY * 64;
+    int total;
+    int pass0 = 0;
+    if (kFirst)
+    {
+        total = a.passes * perPass;
+        pass0 = *a.passBase + a.passOffset;
+    }
+    else
+    {
+        total = *(volatile int*)&a.counts[depth];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(a.rays, kFirst ? (unsigned long long)a.passes * (unsigned long long)W * (unsigned long long)H
+                                 : (unsigned long long)total);
+    const bool final = depth == a.maxDepth;
+    const float missWeight = depth > 0 ? 0.5f : 1.0f;
+
+    bool has = false, exhausted = false, shadow = false;
+    int pixel = 0;
+    uint32_t rng = 0;
+    float thr = 0.f, L = 0.f;
+    float3 extOrg = f3(0.f, 0.f, 0.f), extDir = f3(0.f, 0.f, 1.f);
+    unsigned long long shadowRays = 0;
+    TravRay r;
+    TravState ts;
+    ts.done = true;
+    for (;;)
+    {
+        unsigned idle = __ballot_sync(FULL, !has);
+        if (!exhausted && (__popc(idle) >= kRefillMin || idle == FULL))
+        {
+            int n = __popc(idle);
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&a.fetch[depth], n);
+            base = __shfl_sync(FULL, base, 0);
+            if (base + n >= total) exhausted = true;
+            int i = base + __popc(idle & ltMask);
+            if (!has && i < total)
+            {
+                float3 org, dir;
+                bool ok = true;
+                if (kFirst)
+                {
+                    int pass = i / perPass;
+                    int rr = i - pass * perPass;
+                    int tile = rr >> 6;
+                    int mx, my;
+                    morton8x8(rr & 63, mx, my);
+                    int x = (tile % a.tilesX) * 8 + mx;
+                    int y = (tile / a.tilesX) * 8 + my;
+                    if (x >= W || y >= H)
+                    {
+                        ok = false;
+                    }
+                    else
+                    {
+                        pixel = x + y * W;
+                        rng = rng_seed(pass0 + pass, pixel);
+                        camera_ray(a.cam, x, y, rng, org, dir);
+                        thr = kAlbedo ? 1.0f : a.thrConst;
+                        L = 0.0f;
+                    }
+                }
+                else
+                {
+                    PathRec pr = load_path(a.qin, i);
+                    org = f3(pr.w0.x, pr.w0.y, pr.w0.z);
+                    pixel = __float_as_int(pr.w0.w);
+                    dir = f3(pr.w1.x, pr.w1.y, pr.w1.z);
+                    rng = __float_as_uint(pr.w1.w);
+                    thr = kAlbedo ? __ldcs(a.thrIn + i) : a.thrConst;
+                    L = __ldcs(a.Lin + i);
+                }
+                if (ok)
+                {
+                    has = true;
+                    shadow = false;
+                    trav_setup(r, org, dir);
+                    trav_init(ts, a.scene, FLT_MAX, st);
+                }
+            }
+        }
+        if (__ballot_sync(FULL, has) == 0)
+        {
+            if (exhausted) break;
+            continue;
+        }
+        for (;;)
+        {
+            if (has && !ts.done) trav_step<false>(ts, a.scene, r, 0.0f, st, nullptr, nullptr, shadow);
+            unsigned running = __ballot_sync(FULL, has && !ts.done);
+            if (running == 0) break;
+            if (32 - __popc(running) >= kRefillMin) break;
+        }
+        bool cont = false, end = false;
+        if (has && ts.done)
+        {
+            if (!shadow)
+            {
+                if (ts.triHit < 0)
+                {
+                    L = __fadd_rn(L, __fmul_rn(__fmul_rn(thr, a.sky), missWeight));
+                    end = true;
+                }
+                else if (final)
+                {
+                    end = true;
+                }
+                else
+                {
+                    if (kAlbedo)
+                        thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + ts.primHit) : 0.8f);
+                    else
+                        thr = __fmul_rn(thr, 0.8f);
+                    HitFrame hf = hit_frame(a.scene.tris, ts.triHit, r.org, r.dir, ts.tHit);
+                    float3 so, sd;
+                    sample_bounce(hf, rng, so, sd);          // shadow ray
+                    sample_bounce(hf, rng, extOrg, extDir);  // extension ray
+                    trav_setup(r, so, sd);
+                    trav_init(ts, a.scene, FLT_MAX, st);
+                    shadow = true;
+                    ++shadowRays;
+                }
+            }
+            else
+            {
+                if (ts.triHit < 0) L = __fadd_rn(L, __fmul_rn(__fmul_rn(thr, a.sky), 0.5f));
+                cont = true;
+            }
+        }
+        int o = warp_append(cont, &a.counts[depth + 1]);
+        if (cont)
+        {
+            store_path(a.qout, o, extOrg, pixel, extDir, rng);
+            __stcs(a.Lout + o, L);
+            if (kAlbedo) __stcs(a.thrOut + o, thr);
+            has = false;
+        }
+        else if (end)
+        {
+            red_add_v4(a.accum + pixel, L, L, L, 1.0f);
+            has = false;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) shadowRays += __shfl_down_sync(FULL, shadowRays, off);
+    if (lane == 0 && shadowRays) atomicAdd(a.rays, shadowRays);
+}
+
 template <bool kAnyHit>
 __global__ void __launch_bounds__(128) k_intersect(SceneDev sc, const RayRec* __restrict__ rays, HitRec* __restrict__ hits,
                                                    float* __restrict__ anyOut, int n)
@@ -639,6 +809,20 @@ int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs
         int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);
         kernel<<<grid, cfg.block, shmem, s>>>(a, depth);
     };
+    if (a.Lout)
+    {
+        if (depth == 0)
+        {
+            if (albedo) go(k_bounce_nee<true, true>);
+            else go(k_bounce_nee<true, false>);
+        }
+        else
+        {
+            if (albedo) go(k_bounce_nee<false, true>);
+            else go(k_bounce_nee<false, false>);
+        }
+        return 1;
+    }
     if (depth == 0)
     {
         if (albedo) go(k_bounce<true, true>);

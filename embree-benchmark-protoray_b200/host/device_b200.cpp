@@ -45,8 +45,10 @@ void DeviceB200::initRenderer(const Props& props, Props& stats)
     // the renderer names of the reference's diffuse renderers
     // (render/renderer_factory_single.cpp:56-59, render/device_cuda.cpp:51-93)
     std::string type = props.get("type", "diffuse");
-    if (type != "diffuse" && type != "diffuseFast") throw std::invalid_argument("invalid renderer type");
-    accumulate_ = type == "diffuse";
+    if (type != "diffuse" && type != "diffuseFast" && type != "diffuse2" && type != "diffuse2Fast")
+        throw std::invalid_argument("invalid renderer type");
+    accumulate_ = type == "diffuse" || type == "diffuse2";
+    check(prt_set_integrator(ctx_, type.rfind("diffuse2", 0) == 0 ? PRT_INTEGRATOR_DIFFUSE2 : PRT_INTEGRATOR_DIFFUSE));
     maxDepth_ = props.getInt("maxDepth", 6);   // render/diffuse_integrator_single.h:35
     passesPerFrame_ = props.getInt("sppPerFrame", 1);
     if (passesPerFrame_ < 1) throw std::invalid_argument("sppPerFrame must be positive");

@@ -123,7 +123,7 @@ public:
     std::string getInfo() override;
     void initScene(const std::string& path, const Props& props) override;
     Box3f getSceneBounds() override { return bounds_; }
-    // props: type (diffuse | diffuseFast), maxDepth (default 6), sppPerFrame (default 1)
+    // props: type (diffuse | diffuseFast | diffuse2 | diffuse2Fast), maxDepth (default 6), sppPerFrame (default 1)
     void initRenderer(const Props& props, Props& stats) override;
     // one frame: sppPerFrame passes; stats: mray, ray, spp
     void render(Props& stats) override;

@@ -56,8 +56,10 @@ public:
     void initRenderer(const Props& props, Props& stats)
     {
         std::string type = props.get("type");
-        if (type != "diffuse" && type != "diffuseFast") throw std::invalid_argument("invalid renderer type");
-        accumulate = type == "diffuse";
+        if (type != "diffuse" && type != "diffuseFast" && type != "diffuse2" && type != "diffuse2Fast")
+            throw std::invalid_argument("invalid renderer type");
+        accumulate = type == "diffuse" || type == "diffuse2";
+        check(prt_set_integrator(ctx, type.rfind("diffuse2", 0) == 0 ? PRT_INTEGRATOR_DIFFUSE2 : PRT_INTEGRATOR_DIFFUSE));
         maxDepth = props.get("maxDepth", 6);
         prt_build_stats bs;
         check(prt_build_accel(ctx, &bs));

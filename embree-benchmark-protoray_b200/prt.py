@@ -29,6 +29,7 @@ STATUS_NAMES = {0: "PRT_OK", 1: "PRT_EINVAL", 2: "PRT_ENOMEM", 3: "PRT_ECUDA", 4
 EXPORTS = [
     "prt_create", "prt_destroy", "prt_last_error", "prt_get_info",
     "prt_load_mesh", "prt_load_mesh_file", "prt_get_scene_bounds", "prt_set_albedo", "prt_set_sky",
+    "prt_set_integrator",
     "prt_build_accel", "prt_set_leaf_size", "prt_camera_from_view", "prt_set_camera",
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
@@ -102,6 +103,7 @@ def lib() -> C.CDLL:
         "prt_get_scene_bounds": (ip, [vp, vp, vp]),
         "prt_set_albedo": (ip, [vp, vp, ip]),
         "prt_set_sky": (ip, [vp, fp]),
+        "prt_set_integrator": (ip, [vp, ip]),
         "prt_build_accel": (ip, [vp, C.POINTER(BuildStats)]),
         "prt_set_leaf_size": (ip, [vp, ip]),
         "prt_camera_from_view": (ip, [C.POINTER(View), ip, ip, C.POINTER(Camera)]),
@@ -210,6 +212,13 @@ class Context:
         if not hasattr(albedo, "data_ptr"):
             albedo = np.ascontiguousarray(albedo, np.float32)
         self._check(self.L.prt_set_albedo(self.h, _ptr(albedo), n), "prt_set_albedo")
+
+    def set_integrator(self, name: str):
+        """'diffuse' or 'diffuse2' (next-event estimation)."""
+        kinds = {"diffuse": 0, "diffuse2": 1}
+        if name not in kinds:
+            raise ValueError("invalid renderer type")
+        self._check(self.L.prt_set_integrator(self.h, kinds[name]), "prt_set_integrator")
 
     def set_sky(self, sky: float):
         self._check(self.L.prt_set_sky(self.h, sky), "prt_set_sky")

@@ -133,6 +133,15 @@ int prt_get_scene_bounds(prt_ctx* ctx, float lo[3], float hi[3]);
 int prt_set_albedo(prt_ctx* ctx, const float* albedo, int triCount);
 int prt_set_sky(prt_ctx* ctx, float sky);
 
+/* Integrator of prt_render (render/device_cuda.cpp:51-93 picks the CUDA
+ * renderer by the same names):
+ *   PRT_INTEGRATOR_DIFFUSE   diffuse path tracing (render/diffuse_integrator_single.h:41-69)
+ *   PRT_INTEGRATOR_DIFFUSE2  diffuse path tracing with a shadow ray toward the sky at every
+ *                            bounce and fixed 0.5 MIS weights (render/diffuse2_integrator_single.h:41-90)
+ * The batched, replay/adjoint and allocation-free entry points use PRT_INTEGRATOR_DIFFUSE. */
+enum { PRT_INTEGRATOR_DIFFUSE = 0, PRT_INTEGRATOR_DIFFUSE2 = 1 };
+int prt_set_integrator(prt_ctx* ctx, int integrator);
+
 /* --- acceleration structure (OptixIntersectorStreamCuda ctor, accel/optix/optix_intersector_stream_cuda.cpp:23-75) --- */
 int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats);
 /* Largest leaf of the 8-wide tree, 1..3 triangles, for the next build. */

@@ -96,6 +96,9 @@ class Oracle:
             lib.or_render.restype = C.c_int64
             lib.or_render.argtypes = [C.c_void_p, C.POINTER(OrCamera), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_void_p, C.c_float, C.c_void_p, C.c_int]
+            lib.or_render_ex.restype = C.c_int64
+            lib.or_render_ex.argtypes = [C.c_void_p, C.POINTER(OrCamera), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_int]
             lib.or_render_backward.argtypes = [C.c_void_p, C.POINTER(OrCamera), C.c_int, C.c_int, C.c_int, C.c_int,
                                                C.c_int, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_int]
@@ -176,12 +179,13 @@ class OracleScene:
         return out
 
     def render(self, cam: OrCamera, width: int, height: int, pass0: int, npass: int, max_depth: int,
-               albedo: Optional[np.ndarray] = None, sky: float = 1.0, nthreads: int = 0):
+               albedo: Optional[np.ndarray] = None, sky: float = 1.0, nthreads: int = 0, nee: bool = False):
+        """nee=True evaluates the diffuse2 (next-event estimation) integrator."""
         accum = np.zeros((height, width, 4), np.float64)
         alb = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
-        rays = self.o.lib.or_render(self.h, C.byref(cam), width, height, pass0, npass, max_depth,
-                                    None if alb is None else alb.ctypes.data, C.c_float(sky), accum.ctypes.data,
-                                    nthreads)
+        rays = self.o.lib.or_render_ex(self.h, C.byref(cam), width, height, pass0, npass, max_depth,
+                                       None if alb is None else alb.ctypes.data, C.c_float(sky), accum.ctypes.data,
+                                       nthreads, int(nee))
         return accum, int(rays)
 
     def render_backward(self, cam: OrCamera, width: int, height: int, pass0: int, npass: int, max_depth: int,

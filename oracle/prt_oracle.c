@@ -723,6 +723,56 @@ void or_primary_rays(const or_camera* cam, int W, int H, int pass, float* rays)
         }
 }
 
+/* Diffuse path with next-event estimation toward the sky
+ * (render/diffuse2_integrator_single.h:41-90): at every hit before maxDepth a
+ * cosine-distributed shadow ray is tested for any occluder and, if it
+ * escapes, adds throughput * 0.5; the extension ray adds throughput * 0.5 on
+ * escape after the first bounce and throughput * 1 from the camera (fixed MIS
+ * weights).  Four sample dimensions per bounce: shadow (2), extension (2).
+ * Shadow rays count as rays, as occluded() does in the reference. */
+static double eval_path_nee(const or_scene* s, const or_camera* cam, int W, int H, int x, int y, int pass,
+                            int maxDepth, const float* albedo, double sky, int64_t* rays)
+{
+    int pixel = x + y * W;
+    uint32_t st = or_rng_seed(pass, pixel);
+    double jx, jy, lx, ly;
+    get2d(&st, &jx, &jy);
+    get2d(&st, &lx, &ly);
+    double org[3], dir[3];
+    camera_ray(cam, ((double)x + jx) / (double)W, ((double)y + jy) / (double)H, lx, ly, org, dir);
+    double L = 0.0, thr = 1.0;
+    for (int depth = 0;; ++depth)
+    {
+        or_hit h;
+        int hit = or_intersect(s, org, dir, 0.0, DBL_MAX, &h);
+        (*rays)++;
+        if (!hit)
+        {
+            L += thr * sky * (depth > 0 ? 0.5 : 1.0);
+            break;
+        }
+        if (depth == maxDepth) break;
+        double p[3], eps, Ng[3], U[3], V[3], l[3], sx, sy;
+        or_post_intersect(s, org, dir, h.t, h.primId, p, &eps, Ng);
+        or_make_frame(Ng, U, V);
+        thr *= albedo ? (double)albedo[h.primId] : (double)0.8f;
+        /* shadow ray */
+        get2d(&st, &sx, &sy);
+        or_cosine_sample_hemisphere(sx, sy, l);
+        double so[3], sd[3];
+        for (int k = 0; k < 3; ++k) sd[k] = l[0] * U[k] + l[1] * V[k] + l[2] * Ng[k];
+        for (int k = 0; k < 3; ++k) so[k] = p[k] + eps * sd[k];
+        (*rays)++;
+        if (!or_occluded(s, so, sd, 0.0, DBL_MAX)) L += thr * sky * 0.5;
+        /* extension ray */
+        get2d(&st, &sx, &sy);
+        or_cosine_sample_hemisphere(sx, sy, l);
+        for (int k = 0; k < 3; ++k) dir[k] = l[0] * U[k] + l[1] * V[k] + l[2] * Ng[k];
+        for (int k = 0; k < 3; ++k) org[k] = p[k] + eps * dir[k];
+    }
+    return L;
+}
+
 typedef struct {
     const or_scene* s;
     const or_camera* cam;
@@ -730,6 +780,7 @@ typedef struct {
     const float* albedo;
     double sky;
     double* accum;
+    int nee;
     int64_t rows_rays[1];
     int64_t* rays;          /* per row */
     const double* dL;       /* backward only */
@@ -747,8 +798,10 @@ static void render_row(void* vctx, int y, int worker)
         double* a = c->accum + 4 * ((size_t)y * c->W + x);
         for (int p = 0; p < c->npass; ++p)
         {
-            double v = eval_path(c->s, c->cam, c->W, c->H, x, y, c->pass0 + p, c->maxDepth, c->albedo, c->sky,
-                                 &rays, NULL, NULL, NULL);
+            double v = c->nee ? eval_path_nee(c->s, c->cam, c->W, c->H, x, y, c->pass0 + p, c->maxDepth, c->albedo,
+                                              c->sky, &rays)
+                              : eval_path(c->s, c->cam, c->W, c->H, x, y, c->pass0 + p, c->maxDepth, c->albedo,
+                                          c->sky, &rays, NULL, NULL, NULL);
             a[0] += v; a[1] += v; a[2] += v; a[3] += 1.0;
         }
     }
@@ -758,10 +811,16 @@ static void render_row(void* vctx, int y, int worker)
 int64_t or_render(const or_scene* s, const or_camera* cam, int W, int H, int pass0, int npass, int maxDepth,
                   const float* albedo, float sky, double* accum, int nthreads)
 {
+    return or_render_ex(s, cam, W, H, pass0, npass, maxDepth, albedo, sky, accum, nthreads, 0);
+}
+
+int64_t or_render_ex(const or_scene* s, const or_camera* cam, int W, int H, int pass0, int npass, int maxDepth,
+                     const float* albedo, float sky, double* accum, int nthreads, int nee)
+{
     render_ctx c;
     memset(&c, 0, sizeof(c));
     c.s = s; c.cam = cam; c.W = W; c.H = H; c.pass0 = pass0; c.npass = npass; c.maxDepth = maxDepth;
-    c.albedo = albedo; c.sky = sky; c.accum = accum;
+    c.albedo = albedo; c.sky = sky; c.accum = accum; c.nee = nee;
     c.rays = (int64_t*)calloc((size_t)(H > 0 ? H : 1), sizeof(int64_t));
     par_for(nthreads, H, render_row, &c);
     int64_t total = 0;

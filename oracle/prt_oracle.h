@@ -16,7 +16,8 @@
  *   sampling/random_sampler.h:44-73, math/hash.h:23-72, math/math.h:179
  *   camera/pinhole_camera.h:34-60, camera/thin_lens_camera.h:38-52
  *   math/basis3.h:63-80,128-145, math/vec3.h:409-412
- *   render/renderer_single.h:107-131, render/diffuse_integrator_single.h:41-69
+ *   render/renderer_single.h:107-131, render/diffuse_integrator_single.h:41-69,
+ *   render/diffuse2_integrator_single.h:41-90
  *   geometry/triangle_mesh.cpp:59-153, core/ray.h:40-76
  *   sampling/shape_sampler.h:50-74,114-124
  *   image/accum_buffer.h:130-173 (sum + weight accumulation)
@@ -92,6 +93,12 @@ void or_primary_rays(const or_camera* cam, int width, int height, int pass, floa
 int64_t or_render(const or_scene* s, const or_camera* cam, int width, int height,
                   int pass0, int npass, int maxDepth, const float* albedo, float sky,
                   double* accum, int nthreads);
+
+/* As or_render; nee = 1 evaluates the next-event-estimation integrator of
+ * render/diffuse2_integrator_single.h:41-90 (shadow rays count as rays). */
+int64_t or_render_ex(const or_scene* s, const or_camera* cam, int width, int height,
+                     int pass0, int npass, int maxDepth, const float* albedo, float sky,
+                     double* accum, int nthreads, int nee);
 
 /* FP64 adjoint of or_render with respect to per-triangle albedo and sky.
  * dL_dsum: width*height*3 doubles, the gradient of the loss with respect to

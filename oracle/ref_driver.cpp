@@ -22,6 +22,7 @@
 #include "render/scene.h"
 #include "render/renderer_single.h"
 #include "render/diffuse_integrator_single.h"
+#include "render/diffuse2_integrator_single.h"
 #include "render/diffuse_renderer_stream.h"
 #include "sampling/random_sampler.h"
 #include "sampling/random_sampler_simd.h"
@@ -263,7 +264,7 @@ double ref_scene_build(void* handle, int accel)
 
 // Renders `frames` frames with a reference renderer, one sample per pixel per
 // frame as the reference's render loop does (main/render/render_window.cpp:204-256).
-//   renderer: "diffuse", "diffuseFast", "diffuseStream", "diffuseStreamFast"
+//   renderer: "diffuse", "diffuseFast", "diffuse2", "diffuse2Fast", "diffuseStream", "diffuseStreamFast"
 //   accel:    0 = FP64 oracle BVH, 1 = FP32 SAH BVH
 //   view:     {pos.xyz, angleX, angleY, fovY, radius, focus}
 //   sums:     W*H*4 floats (r,g,b,weight) or NULL
@@ -291,7 +292,18 @@ int ref_render(void* handle, const char* renderer, int accel, int W, int H, int 
 
         ref<const Scene> scene = h->scene;
         ref<Renderer> r;
-        if (type == "diffuse" || type == "diffuseFast")
+        if (type == "diffuse2" || type == "diffuse2Fast")
+        {
+            ref<IntersectorSingle> isect;
+            if (accel == 0) isect = makeRef<OracleIntersector>(h->fp64);
+            else isect = makeRef<FastIntersectorSingle>(&h->bvh);
+            // render/renderer_factory_single.cpp (diffuse2 / diffuse2Fast)
+            if (type == "diffuse2")
+                r = makeRef<RendererSingle<Diffuse2IntegratorSingle<ShadingContext, RandomSampler>, RandomSampler>>(scene, isect, props);
+            else
+                r = makeRef<RendererSingle<Diffuse2IntegratorSingle<SimpleShadingContext, RandomSampler>, RandomSampler, false>>(scene, isect, props);
+        }
+        else if (type == "diffuse" || type == "diffuseFast")
         {
             ref<IntersectorSingle> isect;
             if (accel == 0) isect = makeRef<OracleIntersector>(h->fp64);

@@ -130,6 +130,11 @@ def main():
         out["image_tl_view"] = oracle.view_array(tl)
         out["image_tl_sums"] = sums_tl.astype(np.float32)
         out["image_tl_rays"] = np.array([st_tl["rays"]], np.float64)
+        # next-event-estimation renderer (render/diffuse2_integrator_single.h)
+        sums_d2, st_d2 = rsc.render("diffuse2", view, 64, 64, 4, 3, accel=0)
+        out["image_d2_sums"] = sums_d2.astype(np.float32)
+        out["image_d2_rays"] = np.array([st_d2["rays"]], np.float64)
+        out["image_d2_cfg"] = np.array([64, 64, 4, 3], np.int32)
     np.savez_compressed(OUT, **out)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

@@ -119,6 +119,19 @@ def test_image_matches_reference_renderer(golden, small, small_oracle, oracle_mo
     assert abs(rays - golden["image_tl_rays"][0]) <= 1e-3 * rays
 
 
+def test_nee_image_matches_reference_diffuse2(golden, small, small_oracle, oracle_mod):
+    """The oracle's next-event-estimation path against the reference's own
+    diffuse2 renderer (render/diffuse2_integrator_single.h:41-90)."""
+    mesh, view = small
+    W, H, spp, depth = (int(x) for x in golden["image_d2_cfg"])
+    cam = oracle_mod.Oracle().camera(view, W, H)
+    acc, rays = small_oracle.render(cam, W, H, 0, spp, depth, nee=True)
+    ref = golden["image_d2_sums"]
+    assert np.all(acc[..., 3] == spp)
+    assert _image_rel_error(acc[..., 0], ref[..., 0]) < 1e-3
+    assert abs(rays - golden["image_d2_rays"][0]) <= 1e-3 * rays
+
+
 def test_oracle_adjoint_matches_finite_differences(small, small_oracle, oracle_mod):
     """The FP64 adjoint equals the derivative of the FP64 forward (paths do not
     depend on albedo, so central differences are exact up to rounding)."""

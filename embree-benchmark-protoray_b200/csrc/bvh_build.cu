@@ -575,7 +575,7 @@ inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
         if (e_ != cudaSuccess)                                                                                 \
         {                                                                                                      \
             err = std::string(#x) + ": " + cudaGetErrorString(e_);                                              \
-            status = PRT_ECUDA;                                                                                \
+            status = e_ == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA;                                 \
             goto done;                                                                                         \
         }                                                                                                      \
     } while (0)
@@ -610,24 +610,24 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     BUILD_CHECK(cudaEventCreate(&ev1));
     BUILD_CHECK(cudaEventRecord(ev0, stream));
 
-    BUILD_CHECK(cudaMalloc(&triBox, sizeof(float) * 6 * (size_t)n));
-    BUILD_CHECK(cudaMalloc(&partial, sizeof(float) * 6 * (size_t)boundBlocks));
-    BUILD_CHECK(cudaMalloc(&cbounds, sizeof(float) * 6));
-    BUILD_CHECK(cudaMalloc(&keysA, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(cudaMalloc(&keysB, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(cudaMalloc(&valsA, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(cudaMalloc(&valsB, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(cudaMalloc(&hist, sizeof(uint32_t) * (size_t)histCount));
-    BUILD_CHECK(cudaMalloc(&child, sizeof(int2) * (size_t)std::max(1, nInternal)));
-    BUILD_CHECK(cudaMalloc(&range, sizeof(int2) * (size_t)std::max(1, nInternal)));
-    BUILD_CHECK(cudaMalloc(&parent, sizeof(int) * (size_t)(2 * n)));
-    BUILD_CHECK(cudaMalloc(&flag, sizeof(int) * (size_t)std::max(1, nInternal)));
-    BUILD_CHECK(cudaMalloc(&box, sizeof(float) * 6 * (size_t)(2 * n)));
-    BUILD_CHECK(cudaMalloc(&workA, sizeof(int2) * (size_t)nodeCapacity));
-    BUILD_CHECK(cudaMalloc(&workB, sizeof(int2) * (size_t)nodeCapacity));
-    BUILD_CHECK(cudaMalloc(&counters, sizeof(int) * 4));
-    BUILD_CHECK(cudaMalloc(&out.nodes, sizeof(Bvh8Node) * (size_t)nodeCapacity));
-    BUILD_CHECK(cudaMalloc(&out.tris, sizeof(TriRec) * (size_t)n));
+    BUILD_CHECK(dev_malloc(&triBox, sizeof(float) * 6 * (size_t)n));
+    BUILD_CHECK(dev_malloc(&partial, sizeof(float) * 6 * (size_t)boundBlocks));
+    BUILD_CHECK(dev_malloc(&cbounds, sizeof(float) * 6));
+    BUILD_CHECK(dev_malloc(&keysA, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(dev_malloc(&keysB, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(dev_malloc(&valsA, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(dev_malloc(&valsB, sizeof(uint32_t) * (size_t)n));
+    BUILD_CHECK(dev_malloc(&hist, sizeof(uint32_t) * (size_t)histCount));
+    BUILD_CHECK(dev_malloc(&child, sizeof(int2) * (size_t)std::max(1, nInternal)));
+    BUILD_CHECK(dev_malloc(&range, sizeof(int2) * (size_t)std::max(1, nInternal)));
+    BUILD_CHECK(dev_malloc(&parent, sizeof(int) * (size_t)(2 * n)));
+    BUILD_CHECK(dev_malloc(&flag, sizeof(int) * (size_t)std::max(1, nInternal)));
+    BUILD_CHECK(dev_malloc(&box, sizeof(float) * 6 * (size_t)(2 * n)));
+    BUILD_CHECK(dev_malloc(&workA, sizeof(int2) * (size_t)nodeCapacity));
+    BUILD_CHECK(dev_malloc(&workB, sizeof(int2) * (size_t)nodeCapacity));
+    BUILD_CHECK(dev_malloc(&counters, sizeof(int) * 4));
+    BUILD_CHECK(dev_malloc(&out.nodes, sizeof(Bvh8Node) * (size_t)nodeCapacity));
+    BUILD_CHECK(dev_malloc(&out.tris, sizeof(TriRec) * (size_t)n));
 
     k_tri_boxes<<<boundBlocks, 256, 0, stream>>>(dPos, dIdx, n, triBox, partial);
     k_reduce_bounds<<<1, 256, 0, stream>>>(partial, boundBlocks, cbounds);

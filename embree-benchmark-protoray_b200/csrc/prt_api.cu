@@ -20,6 +20,8 @@
 
 using namespace prt_b200;
 
+long long prt_b200::g_allocFailAfter = -1;
+
 namespace prt_b200 {
 int replay_max_depth();
 int read_counters(unsigned long long* out, bool reset, cudaStream_t s);
@@ -208,9 +210,9 @@ int ensure_queues(prt_ctx* ctx, long long paths, bool withThr, int chains = 1, b
     for (int c = 0; c < nch; ++c)
         for (int i = 0; i < 2; ++i)
         {
-            CK(cudaMalloc(&ctx->q[c][i], sizeof(PathRec) * (size_t)cap));
-            if (thr) CK(cudaMalloc(&ctx->thr[c][i], sizeof(float) * (size_t)cap));
-            if (lq) CK(cudaMalloc(&ctx->Lq[c][i], sizeof(float) * (size_t)cap));
+            CK(dev_malloc(&ctx->q[c][i], sizeof(PathRec) * (size_t)cap));
+            if (thr) CK(dev_malloc(&ctx->thr[c][i], sizeof(float) * (size_t)cap));
+            if (lq) CK(dev_malloc(&ctx->Lq[c][i], sizeof(float) * (size_t)cap));
         }
     ctx->queueCap = cap;
     ctx->queueChains = nch;
@@ -427,8 +429,8 @@ int install_mesh(prt_ctx* ctx, int* dIdx, float* dPos, int nt, int nv, const flo
     int* dBad = nullptr;
     float* dPart = nullptr;
     const int blocks = 128, threads = 256, warps = blocks * threads / 32;
-    cudaError_t e = cudaMalloc(&dBad, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&dPart, sizeof(float) * 6 * warps);
+    cudaError_t e = dev_malloc(&dBad, sizeof(int));
+    if (e == cudaSuccess) e = dev_malloc(&dPart, sizeof(float) * 6 * warps);
     if (e == cudaSuccess) e = cudaMemsetAsync(dBad, 0, sizeof(int), ctx->stream);
     if (e == cudaSuccess && nt)
     {
@@ -553,7 +555,7 @@ int load_mesh_file(prt_ctx* ctx, const char* path, float outLo[3], float outHi[3
         if (pinned) cudaFreeHost(pinned);
         if (dAttr && dAttr != dPos) cudaFree(dAttr);
     };
-    cudaError_t e = cudaHostAlloc(&pinned, std::max<size_t>(idxBytes + attrBytes, 16), cudaHostAllocDefault);
+    cudaError_t e = host_pinned_alloc(&pinned, std::max<size_t>(idxBytes + attrBytes, 16));
     if (e != cudaSuccess) return fail(ctx, PRT_ENOMEM, "cannot allocate pinned staging memory");
     std::fseek(f, 38, SEEK_SET);
     bool ok = std::fread(pinned, 1, idxBytes, f) == idxBytes;
@@ -564,12 +566,12 @@ int load_mesh_file(prt_ctx* ctx, const char* path, float outLo[3], float outHi[3
         cleanup();
         return fail(ctx, PRT_EIO, std::string("read error: ") + path);
     }
-    e = cudaMalloc(&dIdx, std::max<size_t>(idxBytes, 12));
-    if (e == cudaSuccess) e = cudaMalloc(&dPos, sizeof(float) * 3 * (size_t)std::max(vert, 1));
+    e = dev_malloc(&dIdx, std::max<size_t>(idxBytes, 12));
+    if (e == cudaSuccess) e = dev_malloc(&dPos, sizeof(float) * 3 * (size_t)std::max(vert, 1));
     if (e == cudaSuccess)
     {
         if (stride == 3) dAttr = dPos;
-        else e = cudaMalloc(&dAttr, std::max<size_t>(attrBytes, 4));
+        else e = dev_malloc(&dAttr, std::max<size_t>(attrBytes, 4));
     }
     if (e == cudaSuccess && idxBytes) e = cudaMemcpyAsync(dIdx, pinned, idxBytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess && attrBytes)
@@ -653,20 +655,20 @@ int prt_create(int device, prt_ctx** out)
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&ctx->ev0));
     CK(cudaEventCreate(&ctx->ev1));
-    CK(cudaMalloc(&ctx->dPass, sizeof(int)));
+    CK(dev_malloc(&ctx->dPass, sizeof(int)));
     CK(cudaMemset(ctx->dPass, 0, sizeof(int)));
-    CK(cudaMalloc(&ctx->dRays, sizeof(unsigned long long)));
-    CK(cudaMalloc(&ctx->dCounts, sizeof(int) * kCounterStride * kMaxChains));
-    CK(cudaMalloc(&ctx->dFetch, sizeof(int) * kCounterStride * kMaxChains));
+    CK(dev_malloc(&ctx->dRays, sizeof(unsigned long long)));
+    CK(dev_malloc(&ctx->dCounts, sizeof(int) * kCounterStride * kMaxChains));
+    CK(dev_malloc(&ctx->dFetch, sizeof(int) * kCounterStride * kMaxChains));
     CK(cudaEventCreateWithFlags(&ctx->forkEv, cudaEventDisableTiming));
     for (int c = 0; c < kMaxChains; ++c)
     {
         CK(cudaStreamCreateWithFlags(&ctx->side[c], cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&ctx->joinEv[c], cudaEventDisableTiming));
     }
-    CK(cudaMalloc(&ctx->dRay, sizeof(RayRec)));
-    CK(cudaMalloc(&ctx->dHit, sizeof(HitRec)));
-    CK(cudaMalloc(&ctx->dPNg, sizeof(float) * 6));
+    CK(dev_malloc(&ctx->dRay, sizeof(RayRec)));
+    CK(dev_malloc(&ctx->dHit, sizeof(HitRec)));
+    CK(dev_malloc(&ctx->dPNg, sizeof(float) * 6));
     *out = c.release();
     return PRT_OK;
 }
@@ -697,8 +699,8 @@ int prt_load_mesh(prt_ctx* ctx, const int* indices, int triCount, const float* p
     CK(cudaSetDevice(ctx->device));
     int* dIdx = nullptr;
     float* dPos = nullptr;
-    cudaError_t e = cudaMalloc(&dPos, sizeof(float) * 3 * (size_t)std::max(vertCount, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&dIdx, sizeof(int) * 3 * (size_t)std::max(triCount, 1));
+    cudaError_t e = dev_malloc(&dPos, sizeof(float) * 3 * (size_t)std::max(vertCount, 1));
+    if (e == cudaSuccess) e = dev_malloc(&dIdx, sizeof(int) * 3 * (size_t)std::max(triCount, 1));
     if (e == cudaSuccess && vertCount)
         e = cudaMemcpyAsync(dPos, positions, sizeof(float) * 3 * (size_t)vertCount, cudaMemcpyDefault, ctx->stream);
     if (e == cudaSuccess && triCount)
@@ -741,7 +743,7 @@ int prt_set_albedo(prt_ctx* ctx, const float* albedo, int triCount)
         return PRT_OK;
     }
     if (triCount != ctx->nt) return fail(ctx, PRT_EINVAL, "albedo count differs from the triangle count");
-    if (!ctx->dAlbedo) CK(cudaMalloc(&ctx->dAlbedo, sizeof(float) * (size_t)std::max(ctx->nt, 1)));
+    if (!ctx->dAlbedo) CK(dev_malloc(&ctx->dAlbedo, sizeof(float) * (size_t)std::max(ctx->nt, 1)));
     if (ctx->nt)
         CK(cudaMemcpyAsync(ctx->dAlbedo, albedo, sizeof(float) * (size_t)ctx->nt, cudaMemcpyDefault, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -857,7 +859,7 @@ int prt_init_frame(prt_ctx* ctx, int width, int height)
     clear_graphs(ctx);
     cudaFree(ctx->dAccum);
     ctx->dAccum = nullptr;
-    CK(cudaMalloc(&ctx->dAccum, sizeof(float4) * (size_t)width * height));
+    CK(dev_malloc(&ctx->dAccum, sizeof(float4) * (size_t)width * height));
     ctx->W = width;
     ctx->H = height;
     return prt_clear(ctx);
@@ -911,7 +913,7 @@ int prt_read_ldr(prt_ctx* ctx, uint32_t* bgra)
     uint32_t* dOut = nullptr;
     bool dev = is_device_ptr(bgra);
     if (dev) dOut = bgra;
-    else CK(cudaMalloc(&dOut, sizeof(uint32_t) * n));
+    else CK(dev_malloc(&dOut, sizeof(uint32_t) * n));
     ctx->launches += launch_resolve_ldr(ctx->dAccum, dOut, (int)n, ctx->stream);
     CK(cudaGetLastError());
     if (!dev) CK(cudaMemcpyAsync(bgra, dOut, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1113,13 +1115,13 @@ int prt_render_backward(prt_ctx* ctx, int pass0, int spp, int maxDepth, const fl
     if (devL) gL = const_cast<float*>(dL_dsum);
     else
     {
-        CK(cudaMalloc(&gL, sizeof(float) * 3 * npix));
+        CK(dev_malloc(&gL, sizeof(float) * 3 * npix));
         CK(cudaMemcpyAsync(gL, dL_dsum, sizeof(float) * 3 * npix, cudaMemcpyHostToDevice, ctx->stream));
     }
     if (devA) gA = d_albedo;
-    else CK(cudaMalloc(&gA, sizeof(float) * (size_t)std::max(ctx->nt, 1)));
+    else CK(dev_malloc(&gA, sizeof(float) * (size_t)std::max(ctx->nt, 1)));
     if (devS) gS = d_sky;
-    else CK(cudaMalloc(&gS, sizeof(float)));
+    else CK(dev_malloc(&gS, sizeof(float)));
     CK(cudaMemsetAsync(gA, 0, sizeof(float) * (size_t)ctx->nt, ctx->stream));
     CK(cudaMemsetAsync(gS, 0, sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(unsigned long long), ctx->stream));
@@ -1183,7 +1185,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
         if (is_device_ptr(q.accum)) table[(size_t)r].accum = (float4*)q.accum;
         else
         {
-            CK(cudaMalloc(&tmp[(size_t)r], bytes));
+            CK(dev_malloc(&tmp[(size_t)r], bytes));
             table[(size_t)r].accum = tmp[(size_t)r];
             anyTmp = true;
         }
@@ -1193,7 +1195,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
     {
         cudaFree(ctx->dReqs);
         ctx->dReqs = nullptr;
-        CK(cudaMalloc(&ctx->dReqs, sizeof(BatchReq) * (size_t)n));
+        CK(dev_malloc(&ctx->dReqs, sizeof(BatchReq) * (size_t)n));
         ctx->reqCap = n;
         clear_graphs(ctx);
     }
@@ -1287,6 +1289,12 @@ int prt_read_counters(prt_ctx* ctx, long long* out, int n, int reset)
     if (r < 0) return fail(ctx, PRT_ESTATE, "library built without traversal counters (-DPRT_COUNTERS=1)");
     if (r > 0) return fail(ctx, PRT_ECUDA, "counter read-back failed");
     for (int i = 0; i < 6; ++i) out[i] = (long long)c[i];
+    return PRT_OK;
+}
+
+int prt_debug_fail_allocations(long long afterCount)
+{
+    prt_b200::g_allocFailAfter = afterCount < 0 ? -1 : afterCount;
     return PRT_OK;
 }
 

@@ -13,6 +13,34 @@
 
 namespace prt_b200 {
 
+// Every device allocation of the library goes through dev_malloc, so that an
+// out-of-memory condition can be injected on the host (prt_debug_fail_allocations)
+// and every error path tested without exhausting a real GPU.
+extern long long g_allocFailAfter;   // < 0: off; n >= 0: the (n+1)-th allocation from now fails
+
+template <class T>
+inline cudaError_t dev_malloc(T** p, size_t bytes)
+{
+    if (g_allocFailAfter == 0)
+    {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    if (g_allocFailAfter > 0) --g_allocFailAfter;
+    return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
+inline cudaError_t host_pinned_alloc(char** p, size_t bytes)
+{
+    if (g_allocFailAfter == 0)
+    {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    if (g_allocFailAfter > 0) --g_allocFailAfter;
+    return cudaHostAlloc(reinterpret_cast<void**>(p), bytes, cudaHostAllocDefault);
+}
+
 struct Bvh8Device
 {
     Bvh8Node* nodes = nullptr;

@@ -34,7 +34,7 @@ EXPORTS = [
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
-    "prt_render_batch", "prt_read_accel", "prt_read_counters", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
+    "prt_render_batch", "prt_read_accel", "prt_read_counters", "prt_debug_fail_allocations", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
 ]
 
 
@@ -124,6 +124,7 @@ def lib() -> C.CDLL:
         "prt_render_batch": (ip, [vp, C.POINTER(Request), ip, C.POINTER(RenderStats)]),
         "prt_read_accel": (ip, [vp, vp, ip, vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "prt_read_counters": (ip, [vp, vp, ip, ip]),
+        "prt_debug_fail_allocations": (ip, [C.c_longlong]),
         "prt_autotune": (ip, [vp, ip, ip, C.POINTER(Tune)]),
         "prt_set_tune": (ip, [vp, C.POINTER(Tune)]),
         "prt_get_tune": (ip, [vp, C.POINTER(Tune)]),
@@ -143,6 +144,11 @@ def _ptr(a) -> int:
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
     return a.ctypes.data
+
+
+def fail_allocations(after: int) -> None:
+    """Test hook: the (after+1)-th library allocation from now fails (-1: off)."""
+    lib().prt_debug_fail_allocations(after)
 
 
 def camera_from_view(view, width: int, height: int) -> Camera:

@@ -221,6 +221,12 @@ int prt_read_accel(prt_ctx* ctx, void* nodes, int nodeCapacity, void* tris, int 
  * [5] warp triangle-loop iterations.  n >= 6.  Other builds return PRT_ESTATE. */
 int prt_read_counters(prt_ctx* ctx, long long* out, int n, int reset);
 
+/* Failure injection for tests: the (afterCount+1)-th device or pinned-host
+ * allocation made by the library from now on fails as if the GPU were out of
+ * memory (the call reports PRT_ENOMEM); a negative count switches it off.
+ * Process-wide. */
+int prt_debug_fail_allocations(long long afterCount);
+
 /* --- launch configuration --- */
 /* Times candidate bounce-kernel configurations on the current scene/frame
  * and keeps the fastest for later renders. */

@@ -485,22 +485,40 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
         return;
     }
 
-    // header: origin + per-axis power-of-two scale with 255 steps
+    // header: per-axis power-of-two scale s with the node box spanning at most
+    // 253 steps, and origin one step below the box, so every quantized plane
+    // lies at least 2^-8 of a step outside the child box it bounds (the
+    // traversal's plane decode may move a plane inwards by up to 2^-9 step)
     uint32_t ebits[3];
     float scale[3];
+    float origin[3];
     for (int k = 0; k < 3; ++k)
     {
         float ext = nb[3 + k] - nb[k];
         int e = -100;
         if (ext > 0.f)
         {
-            e = (int)ceilf(log2f(ext / 255.0f));
-            while (ldexpf(255.0f, e) < ext) ++e;
+            e = (int)ceilf(log2f(ext / 253.0f));
+            while (ldexpf(253.0f, e) < ext) ++e;
+        }
+        // a step of at least 16 ulps of the coordinates, so that thin or flat
+        // boxes keep distinct planes below and above them
+        float mag = fmaxf(fabsf(nb[k]), fabsf(nb[3 + k]));
+        if (mag > 0.f)
+        {
+            int me;
+            frexpf(mag, &me);
+            e = max(e, me - 20);
         }
         e = max(e, -126);
         e = min(e, 127);
         ebits[k] = (uint32_t)(e + 127);
         scale[k] = ldexpf(1.0f, e);
+        // round the origin down so that it stays at least one step below the box
+        double o = (double)nb[k] - (double)scale[k];
+        float of = (float)o;
+        if ((double)of > o) of = nextafterf(of, -FLT_MAX);
+        origin[k] = of;
     }
     uint8_t meta[8], qlo[3][8], qhi[3][8];
     uint32_t imask = 0;
@@ -517,8 +535,8 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
         const float* b = ref_box(a, ch[i]);
         for (int k = 0; k < 3; ++k)
         {
-            double lo = floor(((double)b[k] - (double)nb[k]) / (double)scale[k]);
-            double hi = ceil(((double)b[3 + k] - (double)nb[k]) / (double)scale[k]);
+            double lo = floor(((double)b[k] - (double)origin[k]) / (double)scale[k] - 1.0 / 256.0);
+            double hi = ceil(((double)b[3 + k] - (double)origin[k]) / (double)scale[k] + 1.0 / 256.0);
             qlo[k][s] = (uint8_t)fmax(0.0, fmin(255.0, lo));
             qhi[k][s] = (uint8_t)fmax(0.0, fmin(255.0, hi));
         }
@@ -555,7 +573,7 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
         return (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
     };
     Bvh8Node node;
-    node.q[0] = make_uint4(__float_as_uint(nb[0]), __float_as_uint(nb[1]), __float_as_uint(nb[2]),
+    node.q[0] = make_uint4(__float_as_uint(origin[0]), __float_as_uint(origin[1]), __float_as_uint(origin[2]),
                            ebits[0] | (ebits[1] << 8) | (ebits[2] << 16) | (imask << 24));
     node.q[1] = make_uint4((uint32_t)childBase, (uint32_t)triBase, pack4(meta), pack4(meta + 4));
     node.q[2] = make_uint4(pack4(qlo[0]), pack4(qlo[0] + 4), pack4(qlo[1]), pack4(qlo[1] + 4));

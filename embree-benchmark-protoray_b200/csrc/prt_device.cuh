@@ -289,6 +289,19 @@ __device__ __forceinline__ float byte_f(uint32_t x, int j)
     return __uint_as_float(__byte_perm(x, 0x4b000000u, 0x7440u + (uint32_t)j)) - 8388608.0f;
 }
 
+// Byte j of x in mantissa bits 8..15 of 1.0f: exactly 1 + q * 2^-15, one
+// byte permute.  A child plane is then fma(u, 2^15 * s * inv, (p - o) * inv -
+// 2^15 * s * inv); the subtraction's rounding moves a plane by at most 2^-9
+// of a quantization step, which the build's 2^-8-step margin covers.
+__device__ __forceinline__ float byte_unit(uint32_t x, int j)
+{
+    return __uint_as_float(__byte_perm(x, 0x3f800000u, 0x7604u + ((uint32_t)j << 4)));
+}
+
+#ifndef PRT_FAST_DECODE
+#define PRT_FAST_DECODE 1
+#endif
+
 // Intersection of the ray with the 8 child boxes of a node.  Returns the hit
 // mask: bits 24..31 internal children (traversal order), bits 0..23 triangles
 // relative to the node's triangle base.
@@ -301,6 +314,15 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
     float sz = __uint_as_float(((e >> 16) & 0xffu) << 23);
     float aix = sx * r.inv.x, aiy = sy * r.inv.y, aiz = sz * r.inv.z;
     float aox = (px - r.org.x) * r.inv.x, aoy = (py - r.org.y) * r.inv.y, aoz = (pz - r.org.z) * r.inv.z;
+    if (PRT_FAST_DECODE)
+    {
+        aix *= 32768.0f;
+        aiy *= 32768.0f;
+        aiz *= 32768.0f;
+        aox -= aix;
+        aoy -= aiy;
+        aoz -= aiz;
+    }
     // For a negative direction component the far plane is the low plane:
     // select per axis which byte array feeds the near / far distance.
     bool nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
@@ -320,12 +342,25 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
         for (int j = 0; j < 4; ++j)
         {
             uint32_t m = (m4 >> (8 * j)) & 0xffu;
-            float tnx = fmaf(byte_f(nearX, j), aix, aox);
-            float tny = fmaf(byte_f(nearY, j), aiy, aoy);
-            float tnz = fmaf(byte_f(nearZ, j), aiz, aoz);
-            float tfx = fmaf(byte_f(farX, j), aix, aox);
-            float tfy = fmaf(byte_f(farY, j), aiy, aoy);
-            float tfz = fmaf(byte_f(farZ, j), aiz, aoz);
+            float tnx, tny, tnz, tfx, tfy, tfz;
+            if (PRT_FAST_DECODE)
+            {
+                tnx = fmaf(byte_unit(nearX, j), aix, aox);
+                tny = fmaf(byte_unit(nearY, j), aiy, aoy);
+                tnz = fmaf(byte_unit(nearZ, j), aiz, aoz);
+                tfx = fmaf(byte_unit(farX, j), aix, aox);
+                tfy = fmaf(byte_unit(farY, j), aiy, aoy);
+                tfz = fmaf(byte_unit(farZ, j), aiz, aoz);
+            }
+            else
+            {
+                tnx = fmaf(byte_f(nearX, j), aix, aox);
+                tny = fmaf(byte_f(nearY, j), aiy, aoy);
+                tnz = fmaf(byte_f(nearZ, j), aiz, aoz);
+                tfx = fmaf(byte_f(farX, j), aix, aox);
+                tfy = fmaf(byte_f(farY, j), aiy, aoy);
+                tfz = fmaf(byte_f(farZ, j), aiz, aoz);
+            }
             float t0 = fmax3(tnx, tny, fmaxf(tnz, tnear));
             float t1 = fmin3(tfx, tfy, fminf(tfz, tfarp));
             bool hit = (m != 0u) && (t0 * 0.9999996f <= t1 * 1.0000004f);
@@ -405,6 +440,11 @@ __device__ __forceinline__ void trav_init(TravState& s, const SceneDev& sc, floa
 // triangles at that moment, so triangle tests run with more lanes together.
 // Off by default: on the 1.4M-triangle terrain at 1080p it measured 1.65
 // Grays/s off vs 1.62 with thresholds of 12 and 16 lanes.
+// Prefetch of the next child node into L1 (on by default if measured faster).
+#ifndef PRT_PREFETCH
+#define PRT_PREFETCH 0
+#endif
+
 #ifndef PRT_POSTPONE_MIN
 #define PRT_POSTPONE_MIN 0
 #endif
@@ -432,6 +472,16 @@ __device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, cons
         uint32_t hits = node_hits(r, q, tnear, s.tHit);
         if (nodeVisits) ++*nodeVisits;
         ng = make_uint2(q[1].x, (hits & 0xff000000u) | (q[0].w >> 24));
+        if (PRT_PREFETCH && (ng.y & 0xff000000u))
+        {
+            // start fetching the child visited next while the triangles are tested
+            uint32_t nb = 31u - __clz(ng.y & 0xff000000u);
+            uint32_t ns = (nb - 24u) ^ r.octinv;
+            uint32_t nidx = ng.x + __popc((ng.y & 0xffu) & ((1u << ns) - 1u));
+            const char* np = reinterpret_cast<const char*>(sc.nodes + nidx);
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(np));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(np + 64));
+        }
         tbits = hits & 0x00ffffffu;
         tbase = q[1].y;
         if (PRT_POSTPONE_MIN > 0 && tbits && (ng.y & 0xff000000u) &&

@@ -329,6 +329,7 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
     uint32_t loX[2] = {q[2].x, q[2].y}, loY[2] = {q[2].z, q[2].w}, loZ[2] = {q[3].x, q[3].y};
     uint32_t hiX[2] = {q[3].z, q[3].w}, hiY[2] = {q[4].x, q[4].y}, hiZ[2] = {q[4].z, q[4].w};
     uint32_t meta[2] = {q[1].z, q[1].w};
+    const uint32_t octinv4 = r.octinv * 0x01010101u;
     uint32_t hits = 0;
     const float tfarp = tfar * 1.0000004f;
 #pragma unroll
@@ -337,11 +338,16 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
         uint32_t nearX = nx ? hiX[h] : loX[h], farX = nx ? loX[h] : hiX[h];
         uint32_t nearY = ny ? hiY[h] : loY[h], farY = ny ? loY[h] : hiY[h];
         uint32_t nearZ = nz ? hiZ[h] : loZ[h], farZ = nz ? loZ[h] : hiZ[h];
+        // per byte: internal children (low 5 meta bits 24..31) put one bit at
+        // 24 + (slot ^ octinv); leaves put their unary triangle count at their
+        // triangle offset; empty slots (meta 0) contribute nothing
         uint32_t m4 = meta[h];
+        uint32_t inner4 = ((m4 & (m4 << 1)) & 0x10101010u) >> 4;           // 1 per internal byte
+        uint32_t index4 = (m4 ^ (octinv4 & (inner4 * 0xffu))) & 0x1f1f1f1fu;
+        uint32_t bits4 = (m4 >> 5) & 0x07070707u;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
-            uint32_t m = (m4 >> (8 * j)) & 0xffu;
             float tnx, tny, tnz, tfx, tfy, tfz;
             if (PRT_FAST_DECODE)
             {
@@ -363,15 +369,8 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
             }
             float t0 = fmax3(tnx, tny, fmaxf(tnz, tnear));
             float t1 = fmin3(tfx, tfy, fminf(tfz, tfarp));
-            bool hit = (m != 0u) && (t0 * 0.9999996f <= t1 * 1.0000004f);
-            if (hit)
-            {
-                uint32_t low = m & 0x1fu;
-                if (low >= 24u)
-                    hits |= 1u << (24u + ((low - 24u) ^ r.octinv));
-                else
-                    hits |= (m >> 5) << low;
-            }
+            // t0 >= tnear >= 0: one relative slack covers rounding on both sides
+            if (t0 <= t1 * 1.0000008f) hits |= ((bits4 >> (8 * j)) & 0xffu) << ((index4 >> (8 * j)) & 0xffu);
         }
     }
     return hits;

@@ -511,7 +511,7 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
             e = max(e, me - 20);
         }
         e = max(e, -126);
-        e = min(e, 127);
+        e = min(e, 100);   // the traversal adds 15 to the biased exponent
         ebits[k] = (uint32_t)(e + 127);
         scale[k] = ldexpf(1.0f, e);
         // round the origin down so that it stays at least one step below the box

@@ -167,9 +167,17 @@ __device__ __forceinline__ void camera_ray(const CameraDev& cam, int x, int y, u
 // octant is s; traversal pops hits in the order of (slot ^ (7 - octant)).
 // ---------------------------------------------------------------------------
 
+// PRT_NODE_PAD pads nodes to 128 bytes (one L1 line each) instead of 80.
+#ifndef PRT_NODE_PAD
+#define PRT_NODE_PAD 0
+#endif
+
 struct Bvh8Node
 {
     uint4 q[5];
+#if PRT_NODE_PAD
+    uint4 pad[3];
+#endif
 };
 
 struct TriRec
@@ -309,16 +317,15 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
 {
     float px = __uint_as_float(q[0].x), py = __uint_as_float(q[0].y), pz = __uint_as_float(q[0].z);
     uint32_t e = q[0].w;
-    float sx = __uint_as_float((e & 0xffu) << 23);
-    float sy = __uint_as_float(((e >> 8) & 0xffu) << 23);
-    float sz = __uint_as_float(((e >> 16) & 0xffu) << 23);
+    // 2^(e-127), times 2^15 for the fast plane decode (the build keeps e <= 100)
+    const uint32_t eb = PRT_FAST_DECODE ? 15u : 0u;
+    float sx = __uint_as_float(((e & 0xffu) + eb) << 23);
+    float sy = __uint_as_float((((e >> 8) & 0xffu) + eb) << 23);
+    float sz = __uint_as_float((((e >> 16) & 0xffu) + eb) << 23);
     float aix = sx * r.inv.x, aiy = sy * r.inv.y, aiz = sz * r.inv.z;
     float aox = (px - r.org.x) * r.inv.x, aoy = (py - r.org.y) * r.inv.y, aoz = (pz - r.org.z) * r.inv.z;
     if (PRT_FAST_DECODE)
     {
-        aix *= 32768.0f;
-        aiy *= 32768.0f;
-        aiz *= 32768.0f;
         aox -= aix;
         aoy -= aiy;
         aoz -= aiz;

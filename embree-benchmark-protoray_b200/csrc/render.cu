@@ -508,6 +508,7 @@ __global__ void k_resolve_ldr(const float4* __restrict__ accum, uint32_t* __rest
 __global__ void k_advance_pass(int* passBase, int spp) { *passBase += spp; }
 
 constexpr int kReplayMaxDepth = 16;
+constexpr int kAggSlots = 1024;   // block-private gradient slots of the adjoint
 
 // Path-replay megakernel: each lane carries whole paths (pass, pixel), from
 // the camera ray to escape or maxDepth.  The forward mode accumulates the
@@ -528,6 +529,21 @@ __global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, f
                                                    int* fetch)
 {
     extern __shared__ uint2 s_stack[];
+    // Block-private accumulation of albedo gradients: a few triangles (a
+    // ground plane) receive most of the contributions, so per-path global
+    // atomics would serialise on them.  Slot = prim mod kAggSlots; a slot
+    // holds one triangle, collisions go straight to global memory.
+    __shared__ int s_key[kBackward ? kAggSlots : 1];
+    __shared__ float s_val[kBackward ? kAggSlots : 1];
+    if (kBackward)
+    {
+        for (int i = threadIdx.x; i < kAggSlots; i += blockDim.x)
+        {
+            s_key[i] = -1;
+            s_val[i] = 0.f;
+        }
+        __syncthreads();
+    }
     TravStack st;
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
@@ -625,8 +641,14 @@ __global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, f
                     float gc = g * c;
                     for (int k = 0; k < np; ++k)
                     {
-                        float al = sc.albedo ? __ldg(sc.albedo + prims[k]) : 0.8f;
-                        atomicAdd(dAlbedo + prims[k], gc / al);
+                        const int pk = prims[k];
+                        float al = sc.albedo ? __ldg(sc.albedo + pk) : 0.8f;
+                        float v = gc / al;
+                        const int slot = pk & (kAggSlots - 1);
+                        int key = s_key[slot];
+                        if (key == -1) key = atomicCAS(&s_key[slot], -1, pk);   // -1: claimed by us
+                        if (key == -1 || key == pk) atomicAdd(&s_val[slot], v);
+                        else atomicAdd(dAlbedo + pk, v);
                     }
                 }
                 has = false;
@@ -643,6 +665,12 @@ __global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, f
     {
         if (kBackward && skyGrad != 0.f) atomicAdd(dSky, skyGrad);
         if (rays) atomicAdd(rays, myRays);
+    }
+    if (kBackward)
+    {
+        __syncthreads();
+        for (int i = threadIdx.x; i < kAggSlots; i += blockDim.x)
+            if (s_key[i] >= 0) atomicAdd(dAlbedo + s_key[i], s_val[i]);
     }
 }
 

@@ -32,7 +32,7 @@ sys.path.insert(0, PKG)
 METRIC = "Mrays/s 1080p 64spp"
 UNIT = "Mrays/s"
 W, H, SPP, DEPTH = 1920, 1080, 64, 5
-ALGO_BYTES_PER_RAY = 192   # compulsory wavefront record traffic per ray
+ALGO_BYTES_PER_RAY = 192   # compulsory wavefront record traffic per ray of the separate-kernel reference design
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -339,6 +339,62 @@ def run_fwd_bwd(prt, torch, device):
             "config": "small scene 82K tris, 512x512, 16 spp, maxDepth 5, per-triangle albedo"}
 
 
+def run_mesh_build(prt, torch, device):
+    """`protoray build` of the terrain scene written as an OBJ (positions and
+    faces, 52 MB): OBJ parse on host threads, GPU mesh build (de-duplication +
+    Morton reorder), .mesh write; beside it the reference's ObjLoader and
+    TriangleMeshBuilder (one host thread each) on the same file, when the
+    reference build is present."""
+    import shutil
+    import tempfile
+    import scenes
+    mesh, _ = scenes.terrain_scene()
+    d = tempfile.mkdtemp(prefix="prt_build_")
+    try:
+        obj = os.path.join(d, "terrain.obj")
+        with open(obj, "w") as f:
+            np.savetxt(f, mesh.positions, fmt="v %.9g %.9g %.9g")
+            np.savetxt(f, mesh.indices + 1, fmt="f %d %d %d")
+        c = prt.Context(device)
+        best = None
+        for _ in range(4):
+            t0 = time.perf_counter()
+            tris, names, _ = prt.load_obj(obj)
+            t1 = time.perf_counter()
+            info = c.build_mesh(tris, names)
+            t2 = time.perf_counter()
+            c.save_built_mesh(os.path.join(d, "terrain.mesh"))
+            t3 = time.perf_counter()
+            r = {"parse_ms": (t1 - t0) * 1e3, "build_device_ms": info["buildMs"], "build_ms": (t2 - t1) * 1e3,
+                 "save_ms": (t3 - t2) * 1e3, "e2e_ms": (t3 - t0) * 1e3}
+            if best is None or r["e2e_ms"] < best["e2e_ms"]:
+                best = r
+        c.close()
+        out = {"triangles": mesh.tri_count, "unique_vertices": info["vertCount"],
+               "obj_mb": round(os.path.getsize(obj) / 1e6, 1), "host_threads": os.cpu_count(),
+               "gpu": {k: round(v, 2) for k, v in best.items()},
+               "build_mtris_per_s": round(mesh.tri_count / best["build_ms"] / 1e3, 1),
+               "build_device_mtris_per_s": round(mesh.tri_count / best["build_device_ms"] / 1e3, 1)}
+        ref_so = os.path.join(ROOT, "oracle", "_ref", "libprotoray_ref.so")
+        if os.path.exists(ref_so):
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            R = oracle.Reference()
+            t0 = time.perf_counter()
+            rt, rn = R.load_obj(obj)
+            t1 = time.perf_counter()
+            build_ms = R.build_soup(rt, rn, os.path.join(d, "terrain_ref.mesh"))
+            t2 = time.perf_counter()
+            out["reference"] = {"parse_ms": round((t1 - t0) * 1e3, 1), "build_ms": round(build_ms, 1),
+                                "e2e_ms": round((t2 - t0) * 1e3, 1),
+                                "kind": "reference ObjLoader + TriangleMeshBuilder compiled from source, 1 thread"}
+            out["speedup_build"] = round(build_ms / best["build_ms"], 1)
+            out["speedup_e2e"] = round((t2 - t0) * 1e3 / best["e2e_ms"], 1)
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def main():
     global W, H, SPP
     ap = argparse.ArgumentParser()
@@ -446,6 +502,7 @@ def main():
     if rank == 0 and not args.no_extras:
         extras["batched"] = run_batch(prt, torch, local)
         extras["differentiable"] = run_fwd_bwd(prt, torch, local)
+        extras["mesh_build"] = run_mesh_build(prt, torch, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

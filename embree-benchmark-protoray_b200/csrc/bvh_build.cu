@@ -28,12 +28,6 @@ namespace prt_b200 {
 
 namespace {
 
-constexpr int kSortBlock = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortBlock * kSortItems;
-constexpr int kRadixBits = 4;
-constexpr int kRadix = 1 << kRadixBits;
-
 struct Box6
 {
     float lo[3], hi[3];
@@ -142,138 +136,7 @@ __global__ void k_morton(const float* __restrict__ triBox, int nt, const float* 
     vals[p] = (uint32_t)p;
 }
 
-// --- 3. radix sort (stable LSD, 4-bit digits) -----------------------------
-
-__global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift,
-                                                        uint32_t* __restrict__ hist, int nblocks)
-{
-    __shared__ uint32_t h[kRadix];
-    if (threadIdx.x < kRadix) h[threadIdx.x] = 0;
-    __syncthreads();
-    int base = blockIdx.x * kSortTile;
-    for (int k = 0; k < kSortItems; ++k)
-    {
-        int i = base + k * kSortBlock + threadIdx.x;
-        if (i < n) atomicAdd(&h[(keys[i] >> shift) & (kRadix - 1)], 1u);
-    }
-    __syncthreads();
-    if (threadIdx.x < kRadix) hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
-}
-
-// exclusive scan of hist (kRadix * nblocks entries, digit-major) in one block
-__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* __restrict__ hist, int count)
-{
-    __shared__ uint32_t part[1024];
-    int per = (count + 1023) / 1024;
-    int b0 = threadIdx.x * per, b1 = min(count, b0 + per);
-    uint32_t sum = 0;
-    for (int i = b0; i < b1; ++i) sum += hist[i];
-    part[threadIdx.x] = sum;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1)
-    {
-        uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
-    }
-    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
-    for (int i = b0; i < b1; ++i)
-    {
-        uint32_t v = hist[i];
-        hist[i] = run;
-        run += v;
-    }
-}
-
-// Each thread owns kSortItems consecutive keys of the tile; per-thread digit
-// counts are scanned block-wide in (digit, thread) order, which gives every
-// key its stable rank within the tile.
-__global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint32_t* __restrict__ keysIn,
-                                                           const uint32_t* __restrict__ valsIn, uint32_t* __restrict__ keysOut,
-                                                           uint32_t* __restrict__ valsOut, int n, int shift,
-                                                           const uint32_t* __restrict__ hist, int nblocks)
-{
-    __shared__ uint32_t cnt[kRadix * kSortBlock];   // [digit][thread]
-    __shared__ uint32_t warpSum[kSortBlock / 32];
-    __shared__ uint32_t digitStart[kRadix];
-    const int t = threadIdx.x;
-    const int base = blockIdx.x * kSortTile + t * kSortItems;
-    uint32_t key[kSortItems], val[kSortItems];
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k)
-    {
-        int i = base + k;
-        key[k] = i < n ? keysIn[i] : 0xffffffffu;
-        val[k] = i < n ? valsIn[i] : 0u;
-    }
-#pragma unroll
-    for (int d = 0; d < kRadix; ++d) cnt[d * kSortBlock + t] = 0;
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k)
-        if (base + k < n) cnt[((key[k] >> shift) & (kRadix - 1)) * kSortBlock + t]++;
-    __syncthreads();
-    // block-wide exclusive scan over cnt[] (kRadix * kSortBlock entries):
-    // thread t scans entries [t*kRadix, (t+1)*kRadix) sequentially
-    uint32_t local[kRadix];
-    uint32_t sum = 0;
-#pragma unroll
-    for (int j = 0; j < kRadix; ++j)
-    {
-        local[j] = cnt[t * kRadix + j];
-        sum += local[j];
-    }
-    // scan of per-thread sums
-    uint32_t x = sum;
-    const int lane = t & 31, warp = t >> 5;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1)
-    {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
-        if (lane >= off) x += y;
-    }
-    if (lane == 31) warpSum[warp] = x;
-    __syncthreads();
-    if (warp == 0)
-    {
-        uint32_t w = lane < kSortBlock / 32 ? warpSum[lane] : 0u;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1)
-        {
-            uint32_t y = __shfl_up_sync(0xffffffffu, w, off);
-            if (lane >= off) w += y;
-        }
-        if (lane < kSortBlock / 32) warpSum[lane] = w;
-    }
-    __syncthreads();
-    uint32_t excl = x - sum + (warp ? warpSum[warp - 1] : 0u);
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kRadix; ++j)
-    {
-        cnt[t * kRadix + j] = excl;
-        excl += local[j];
-    }
-    __syncthreads();
-    if (t < kRadix) digitStart[t] = cnt[t * kSortBlock];
-    __syncthreads();
-    uint32_t seen[kRadix];
-#pragma unroll
-    for (int d = 0; d < kRadix; ++d) seen[d] = 0;
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k)
-    {
-        if (base + k >= n) continue;
-        uint32_t d = (key[k] >> shift) & (kRadix - 1);
-        uint32_t rankInTile = cnt[d * kSortBlock + t] + seen[d];
-#pragma unroll
-        for (int dd = 0; dd < kRadix; ++dd)
-            if (dd == (int)d) seen[dd]++;
-        uint32_t dst = hist[d * nblocks + blockIdx.x] + (rankInTile - digitStart[d]);
-        keysOut[dst] = key[k];
-        valsOut[dst] = val[k];
-    }
-}
+// --- 3. radix sort: radix_sort_pairs (sort_scan.cu) -------------------------
 
 // --- 4. Karras binary radix tree --------------------------------------------
 
@@ -608,8 +471,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
 
     const int n = nt;
     const int nInternal = n > 1 ? n - 1 : 0;
-    const int sortBlocks = div_up(n, kSortTile);
-    const int histCount = kRadix * sortBlocks;
+    const size_t histCount = radix_sort_hist_entries(n);
     const int boundBlocks = std::min(1024, div_up(n, 256));
     const int nodeCapacity = std::max(1, nInternal);
 
@@ -650,14 +512,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     k_tri_boxes<<<boundBlocks, 256, 0, stream>>>(dPos, dIdx, n, triBox, partial);
     k_reduce_bounds<<<1, 256, 0, stream>>>(partial, boundBlocks, cbounds);
     k_morton<<<div_up(n, 256), 256, 0, stream>>>(triBox, n, cbounds, keysA, valsA);
-    for (int shift = 0; shift < 32; shift += kRadixBits)
-    {
-        k_sort_hist<<<sortBlocks, kSortBlock, 0, stream>>>(keysA, n, shift, hist, sortBlocks);
-        k_sort_scan<<<1, 1024, 0, stream>>>(hist, histCount);
-        k_sort_scatter<<<sortBlocks, kSortBlock, 0, stream>>>(keysA, valsA, keysB, valsB, n, shift, hist, sortBlocks);
-        std::swap(keysA, keysB);
-        std::swap(valsA, valsB);
-    }
+    radix_sort_pairs(keysA, valsA, keysB, valsB, hist, n, 30, stream);
     if (nInternal > 0)
     {
         k_karras<<<div_up(nInternal, 256), 256, 0, stream>>>(keysA, n, child, range, parent);

@@ -6,6 +6,7 @@
 // context's own stream; the only host synchronisations are at the end of a
 // render call (ray-count read-back) and in the build's level loop.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -93,6 +94,9 @@ struct prt_ctx
     // batch scratch
     BatchReq* dReqs = nullptr;
     int reqCap = 0;
+
+    // mesh built from a triangle soup (prt_build_mesh)
+    BuiltMesh builtMesh;
 
     LaunchCfg cfg;
     long long launches = 0;
@@ -629,6 +633,7 @@ prt_ctx::~prt_ctx()
     cudaFree(dHit);
     cudaFree(dPNg);
     cudaFree(dReqs);
+    builtMesh.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1382,6 +1387,119 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
         best->concurrentWaves = bestCfg.chains;
         best->mray = bestMray;
     }
+    return PRT_OK;
+}
+
+int prt_build_mesh(prt_ctx* ctx, const prt_soup_triangle* tris, int triCount, const char* const* materialNames,
+                   int materialCount, prt_mesh_info* info)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (triCount < 0 || (triCount > 0 && !tris)) return fail(ctx, PRT_EINVAL, "invalid soup");
+    if (materialCount < 0 || (materialCount > 0 && !materialNames)) return fail(ctx, PRT_EINVAL, "invalid material names");
+    for (int i = 0; i < materialCount; ++i)
+        if (!materialNames[i]) return fail(ctx, PRT_EINVAL, "null material name");
+    CK(cudaSetDevice(ctx->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    double buildMs = 0;
+    int st = build_mesh_gpu(tris, triCount, ctx->stream, ctx->builtMesh, ctx->err, &buildMs, &ctx->launches);
+    if (st != PRT_OK) return st;
+    const auto t1 = std::chrono::steady_clock::now();
+    BuiltMesh& m = ctx->builtMesh;
+    m.names.assign(materialNames, materialNames + materialCount);
+    if (info)
+    {
+        info->triCount = m.triCount;
+        info->vertCount = m.vertCount;
+        info->hasNormals = m.hasNormals;
+        info->hasTexcoords = m.hasTexcoords;
+        info->hasMaterials = m.hasMaterials;
+        std::memcpy(info->boundsLo, m.lo, sizeof(m.lo));
+        std::memcpy(info->boundsHi, m.hi, sizeof(m.hi));
+        info->buildMs = buildMs;
+        info->totalMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    return PRT_OK;
+}
+
+int prt_read_built_mesh(prt_ctx* ctx, int* indices, int* materialIds, float* positions, float* normals, float* texcoords)
+{
+    if (!ctx) return PRT_EINVAL;
+    const BuiltMesh& m = ctx->builtMesh;
+    if (!m.valid) return fail(ctx, PRT_ESTATE, "no mesh has been built");
+    if ((m.triCount && (!indices || !materialIds)) || (m.vertCount && !positions) ||
+        (m.vertCount && m.hasNormals && !normals) || (m.vertCount && m.hasTexcoords && !texcoords))
+        return fail(ctx, PRT_EINVAL, "null output array");
+    CK(cudaSetDevice(ctx->device));
+    if (m.triCount)
+    {
+        CK(cudaMemcpyAsync(indices, m.idx, sizeof(int) * 3 * (size_t)m.triCount, cudaMemcpyDefault, ctx->stream));
+        CK(cudaMemcpyAsync(materialIds, m.mat, sizeof(int) * (size_t)m.triCount, cudaMemcpyDefault, ctx->stream));
+    }
+    if (m.vertCount)
+    {
+        // de-interleave with strided copies: position, normal and texcoord columns
+        const size_t pitch = sizeof(float) * m.stride;
+        CK(cudaMemcpy2DAsync(positions, 12, m.attr, pitch, 12, m.vertCount, cudaMemcpyDefault, ctx->stream));
+        if (m.hasNormals)
+            CK(cudaMemcpy2DAsync(normals, 12, m.attr + 3, pitch, 12, m.vertCount, cudaMemcpyDefault, ctx->stream));
+        if (m.hasTexcoords)
+            CK(cudaMemcpy2DAsync(texcoords, 8, m.attr + (m.hasNormals ? 6 : 3), pitch, 8, m.vertCount,
+                                 cudaMemcpyDefault, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+int prt_save_built_mesh(prt_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return PRT_EINVAL;
+    const BuiltMesh& m = ctx->builtMesh;
+    if (!m.valid) return fail(ctx, PRT_ESTATE, "no mesh has been built");
+    CK(cudaSetDevice(ctx->device));
+    // the blob in one pinned buffer: header, indices, material ids, attributes, names
+    const size_t idxBytes = 12 * (size_t)m.triCount, matBytes = 4 * (size_t)m.triCount;
+    const size_t attrBytes = sizeof(float) * m.stride * (size_t)m.vertCount;
+    size_t namesBytes = 4;
+    for (const std::string& s : m.names) namesBytes += 4 + s.size();
+    const size_t total = 38 + idxBytes + matBytes + attrBytes + namesBytes;
+    char* buf = nullptr;
+    CK(host_pinned_alloc(&buf, total));
+    struct Freer
+    {
+        char* p;
+        ~Freer() { cudaFreeHost(p); }
+    } freer{buf};
+    const int id = 0x04df8666, tri = m.triCount, vert = m.vertCount;
+    std::memcpy(buf, &id, 4);
+    std::memcpy(buf + 4, m.lo, 12);
+    std::memcpy(buf + 16, m.hi, 12);
+    std::memcpy(buf + 28, &tri, 4);
+    std::memcpy(buf + 32, &vert, 4);
+    buf[36] = m.hasNormals ? 1 : 0;
+    buf[37] = m.hasTexcoords ? 1 : 0;
+    char* at = buf + 38;
+    if (idxBytes) CK(cudaMemcpyAsync(at, m.idx, idxBytes, cudaMemcpyDeviceToHost, ctx->stream));
+    at += idxBytes;
+    if (matBytes) CK(cudaMemcpyAsync(at, m.mat, matBytes, cudaMemcpyDeviceToHost, ctx->stream));
+    at += matBytes;
+    if (attrBytes) CK(cudaMemcpyAsync(at, m.attr, attrBytes, cudaMemcpyDeviceToHost, ctx->stream));
+    at += attrBytes;
+    const int count = (int)m.names.size();
+    std::memcpy(at, &count, 4);
+    at += 4;
+    for (const std::string& s : m.names)
+    {
+        const int len = (int)s.size();
+        std::memcpy(at, &len, 4);
+        std::memcpy(at + 4, s.data(), s.size());
+        at += 4 + s.size();
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(ctx, PRT_EIO, std::string("cannot create ") + path);
+    const bool ok = std::fwrite(buf, 1, total, f) == total;
+    const bool closed = std::fclose(f) == 0;
+    if (!ok || !closed) return fail(ctx, PRT_EIO, std::string("write error: ") + path);
     return PRT_OK;
 }
 

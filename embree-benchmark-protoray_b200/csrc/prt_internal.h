@@ -69,6 +69,48 @@ struct BuildInfo
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
                std::string& err, BuildInfo* info, int leafMax);
 
+// Sort and scan primitives (sort_scan.cu).  radix_sort_pairs sorts (key, value)
+// pairs stably on key bits [0, bits); the sorted pairs end in keys/vals (the
+// pointers are swapped with the temporaries as needed).  hist needs
+// radix_sort_hist_entries(n) words.  exclusive_scan_u32 writes the exclusive
+// prefix sums of in[0, n) to out and the total to sums[scan_sums_entries(n) - 1].
+// Both return the number of launches.
+size_t radix_sort_hist_entries(int n);
+int radix_sort_pairs(uint32_t*& keys, uint32_t*& vals, uint32_t*& keysTmp, uint32_t*& valsTmp, uint32_t* hist, int n,
+                     int bits, cudaStream_t stream);
+size_t scan_sums_entries(int n);
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t* sums, int n, cudaStream_t stream);
+
+// An indexed mesh built from a triangle soup on the device (mesh_build.cu).
+struct BuiltMesh
+{
+    int* idx = nullptr;     // [3 * triCount]
+    int* mat = nullptr;     // [triCount]
+    float* attr = nullptr;  // [vertCount * stride]: position [, normal] [, texcoord], as in the .mesh blob
+    int triCount = 0, vertCount = 0, stride = 3;
+    bool hasNormals = false, hasTexcoords = false, hasMaterials = false;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    std::vector<std::string> names;
+    bool valid = false;
+
+    void release()
+    {
+        cudaFree(idx);
+        cudaFree(mat);
+        cudaFree(attr);
+        idx = mat = nullptr;
+        attr = nullptr;
+        triCount = vertCount = 0;
+        valid = false;
+        names.clear();
+    }
+};
+
+// TriangleMeshBuilder on the device; hostTris may be host or device memory.
+// On success `out` owns the mesh (names are left to the caller).
+int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream, BuiltMesh& out, std::string& err,
+                   double* buildMs, long long* launches);
+
 // Arguments of one wave of the wavefront renderer.
 struct WaveArgs
 {

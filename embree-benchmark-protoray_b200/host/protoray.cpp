@@ -1,5 +1,6 @@
 // protoray — command line of the B200 path tracer with the reference's
-// `protoray render` interface (main/main.cpp:43-69, main/render/render.cpp):
+// `protoray render` and `protoray build` interfaces (main/main.cpp:43-69,
+// main/render/render.cpp, main/build/build.cpp):
 //
 //   protoray render scene.mesh [-r diffuse|diffuseFast] [-spp N] [-size W,H]
 //       [-maxDepth D] [-dev b200] [-view K] [-benchmark PREFIX | -o PREFIX]
@@ -14,6 +15,16 @@
 // (<prefix>.csv) and the image (<prefix>.ppm) (render_window.cpp:145-162,
 // 227-255).  Only offscreen rendering exists (the reference's window mode is
 // unsupported too, main/render/window.cpp:129-133).
+//
+//   protoray build input.obj|input.mesh [-o output] [-t mesh] [-threads N]
+//
+// parses the OBJ on host threads and builds the indexed mesh on the GPU
+// (prt_soup_load_obj + prt_build_mesh), then writes the .mesh blob; the output
+// defaults to the input name with its extension replaced by the type
+// (build.cpp:84-85).  A .mesh input is read and written back.  Unlike the
+// reference, which ignores ObjLoader::load's result and writes an empty mesh
+// for a malformed OBJ (build.cpp:100-104), an OBJ error ends the command with
+// status 1 and no output file.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -311,25 +322,135 @@ int main_render(const std::vector<std::string>& args)
     return 0;
 }
 
+// .mesh re-save (build.cpp:92-96): the blob is parsed (geometry/triangle_mesh.cpp:305-320)
+// and written back without anything that follows it.
+int resave_mesh(const std::string& input, const std::string& output)
+{
+    std::ifstream f(input, std::ios::binary);
+    if (!f) throw std::runtime_error("cannot open " + input);
+    std::vector<char> data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    auto need = [&](size_t at, size_t n) {
+        if (at + n > data.size()) throw std::runtime_error("unexpected end of stream: " + input);
+    };
+    auto geti = [&](size_t at) {
+        int v;
+        need(at, 4);
+        std::memcpy(&v, &data[at], 4);
+        return v;
+    };
+    if (geti(0) != 0x04df8666) throw std::runtime_error("file has wrong blob ID: " + input);
+    need(0, 38);
+    const int tri = geti(28), vert = geti(32);
+    if (tri < 0 || vert < 0) throw std::runtime_error("negative element count: " + input);
+    const int stride = 3 + (data[36] ? 3 : 0) + (data[37] ? 2 : 0);
+    size_t at = 38 + 16 * (size_t)tri + 4 * (size_t)stride * vert;
+    const int names = geti(at);
+    at += 4;
+    for (int i = 0; i < names; ++i)
+    {
+        const int len = geti(at);
+        if (len < 0) throw std::runtime_error("negative string length: " + input);
+        need(at + 4, (size_t)len);
+        at += 4 + (size_t)len;
+    }
+    std::ofstream o(output, std::ios::binary);
+    if (!o.write(data.data(), (std::streamsize)at)) throw std::runtime_error("cannot write " + output);
+    return 0;
+}
+
+int main_build(const std::vector<std::string>& args)
+{
+    // build.log beside the working directory, as the reference (build.cpp:41)
+    std::ofstream log("build.log");
+    auto say = [&](const std::string& m) {
+        std::cout << m << std::endl;
+        log << m << std::endl;
+    };
+    std::string type = "mesh", input, output;
+    int threads = 0;
+    for (const Option& opt : parse_args(args))
+    {
+        if (opt.name.empty())
+        {
+            if (!input.empty()) throw std::invalid_argument("Multiple inputs");
+            input = opt.value;
+        }
+        else if (opt.name == "o")
+        {
+            if (!output.empty()) throw std::invalid_argument("Multiple outputs");
+            output = opt.value;
+        }
+        else if (opt.name == "t")
+            type = opt.value;
+        else if (opt.name == "threads")
+            threads = std::stoi(opt.value);
+        else
+            say("Option: " + opt.name + " = " + opt.value);
+    }
+    if (output.empty()) output = input.substr(0, input.find_last_of('.')) + "." + type;
+    const std::string ext = input.substr(input.find_last_of('.') + 1);
+    if (ext != "mesh" && ext != "obj")
+    {
+        std::cerr << "Error: Unsupported input format" << std::endl;
+        return 1;
+    }
+    if (type != "mesh")
+    {
+        std::cerr << "Error: Invalid type" << std::endl;
+        return 1;
+    }
+    if (ext == "mesh") return resave_mesh(input, output);
+
+    const auto t0 = std::chrono::steady_clock::now();
+    prt_soup* soup = nullptr;
+    char err[512];
+    if (prt_soup_load_obj(input.c_str(), threads, &soup, err, sizeof(err)) != PRT_OK)
+        throw std::runtime_error(std::string(err) + " (" + input + ")");
+    struct SoupFree
+    {
+        prt_soup* s;
+        ~SoupFree() { prt_soup_free(s); }
+    } soupFree{soup};
+    const auto t1 = std::chrono::steady_clock::now();
+    int triCount = 0, nameCount = 0, degenerate = 0;
+    prt_soup_info(soup, &triCount, &nameCount, &degenerate);
+    if (degenerate > 0) say("Removed " + std::to_string(degenerate) + " degenerate triangles");
+    std::vector<const char*> names((size_t)nameCount);
+    for (int i = 0; i < nameCount; ++i) names[(size_t)i] = prt_soup_material_name(soup, i);
+
+    DeviceB200 dev(0);
+    prt_mesh_info info;
+    int st = prt_build_mesh(dev.handle(), prt_soup_triangles(soup), triCount, names.data(), nameCount, &info);
+    if (st != PRT_OK) throw std::runtime_error(prt_last_error(dev.handle()));
+    st = prt_save_built_mesh(dev.handle(), output.c_str());
+    if (st != PRT_OK) throw std::runtime_error(prt_last_error(dev.handle()));
+    const double parseMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    say("Built " + output + ": " + std::to_string(info.triCount) + " triangles, " + std::to_string(info.vertCount) +
+        " unique vertices (OBJ " + std::to_string(parseMs) + " ms, build " + std::to_string(info.buildMs) + " ms)");
+    return 0;
+}
+
 } // namespace
 
 int main(int argc, char** argv)
 {
     std::vector<std::string> args(argv + 1, argv + argc);
-    if (args.empty() || (args[0] != "render"))
+    if (args.empty() || (args[0] != "render" && args[0] != "build"))
     {
         std::cout << "Usage: protoray render scene.mesh [options]" << std::endl;
+        std::cout << "       protoray build input.obj [-o output.mesh]" << std::endl;
         return args.empty() ? 0 : 1;
     }
+    const std::string cmd = args[0];
     args.erase(args.begin());
     if (args.empty())
     {
-        std::cout << "Usage: protoray render [options]" << std::endl;
+        std::cout << "Usage: protoray " << cmd << " [options]" << std::endl;
         return 0;
     }
     try
     {
-        return main_render(args);
+        return cmd == "build" ? main_build(args) : main_render(args);
     }
     catch (const std::exception& e)
     {

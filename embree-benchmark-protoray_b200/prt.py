@@ -35,6 +35,8 @@ EXPORTS = [
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
     "prt_render_batch", "prt_read_accel", "prt_read_counters", "prt_debug_fail_allocations", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
+    "prt_soup_load_obj", "prt_soup_info", "prt_soup_triangles", "prt_soup_material_name", "prt_soup_free",
+    "prt_build_mesh", "prt_read_built_mesh", "prt_save_built_mesh",
 ]
 
 
@@ -74,6 +76,17 @@ class RenderStats(C.Structure):
 class Request(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("width", C.c_int), ("height", C.c_int),
                 ("spp", C.c_int), ("maxDepth", C.c_int), ("accum", C.c_void_p)]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [("triCount", C.c_int), ("vertCount", C.c_int), ("hasNormals", C.c_int), ("hasTexcoords", C.c_int),
+                ("hasMaterials", C.c_int), ("boundsLo", C.c_float * 3), ("boundsHi", C.c_float * 3),
+                ("buildMs", C.c_double), ("totalMs", C.c_double)]
+
+
+# prt_soup_triangle: three {pos, normal, tex} vertices and a material id, 100 bytes
+SOUP_VERTEX_DTYPE = np.dtype([("pos", "<f4", 3), ("normal", "<f4", 3), ("tex", "<f4", 2)])
+SOUP_DTYPE = np.dtype([("v", SOUP_VERTEX_DTYPE, 3), ("matId", "<i4")])
 
 
 class Tune(C.Structure):
@@ -130,6 +143,14 @@ def lib() -> C.CDLL:
         "prt_get_tune": (ip, [vp, C.POINTER(Tune)]),
         "prt_render_noalloc": (ip, [vp, C.POINTER(Camera), ip, ip, ip, ip, ip, vp, C.POINTER(C.c_longlong)]),
         "prt_launch_count": (C.c_longlong, [vp]),
+        "prt_soup_load_obj": (ip, [C.c_char_p, ip, C.POINTER(vp), C.c_char_p, ip]),
+        "prt_soup_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "prt_soup_triangles": (vp, [vp]),
+        "prt_soup_material_name": (C.c_char_p, [vp, ip]),
+        "prt_soup_free": (None, [vp]),
+        "prt_build_mesh": (ip, [vp, vp, ip, C.POINTER(C.c_char_p), ip, C.POINTER(MeshInfo)]),
+        "prt_read_built_mesh": (ip, [vp, vp, vp, vp, vp, vp]),
+        "prt_save_built_mesh": (ip, [vp, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -149,6 +170,29 @@ def _ptr(a) -> int:
 def fail_allocations(after: int) -> None:
     """Test hook: the (after+1)-th library allocation from now fails (-1: off)."""
     lib().prt_debug_fail_allocations(after)
+
+
+def load_obj(path: str, threads: int = 0):
+    """OBJ -> triangle soup (ObjLoader::load, main/build/obj_loader.cpp:35-53).
+
+    Returns (triangles as a SOUP_DTYPE array, material names, dropped
+    degenerate triangles); raises PrtError on a malformed file."""
+    L = lib()
+    h = C.c_void_p()
+    err = C.create_string_buffer(512)
+    st = L.prt_soup_load_obj(path.encode(), threads, C.byref(h), err, 512)
+    if st != PRT_OK:
+        raise PrtError(st, err.value.decode())
+    try:
+        n, m, d = C.c_int(), C.c_int(), C.c_int()
+        L.prt_soup_info(h, C.byref(n), C.byref(m), C.byref(d))
+        tris = np.zeros(n.value, SOUP_DTYPE)
+        if n.value:
+            C.memmove(tris.ctypes.data, L.prt_soup_triangles(h), n.value * SOUP_DTYPE.itemsize)
+        names = [L.prt_soup_material_name(h, i).decode() for i in range(m.value)]
+        return tris, names, d.value
+    finally:
+        L.prt_soup_free(h)
 
 
 def camera_from_view(view, width: int, height: int) -> Camera:
@@ -347,6 +391,37 @@ class Context:
     def launch_count(self) -> int:
         return int(self.L.prt_launch_count(self.h))
 
+    def build_mesh(self, tris: np.ndarray, names: Sequence[str]) -> Dict[str, object]:
+        """TriangleMeshBuilder on the GPU (prt_build_mesh); the mesh stays on
+        the device until read_built_mesh / save_built_mesh."""
+        tris = np.ascontiguousarray(tris, SOUP_DTYPE)
+        arr = (C.c_char_p * max(1, len(names)))(*[s.encode() for s in names])
+        info = MeshInfo()
+        self._check(self.L.prt_build_mesh(self.h, tris.ctypes.data if len(tris) else None, len(tris), arr, len(names),
+                                          C.byref(info)), "prt_build_mesh")
+        self._mesh_info = info
+        return {"triCount": info.triCount, "vertCount": info.vertCount, "hasNormals": bool(info.hasNormals),
+                "hasTexcoords": bool(info.hasTexcoords), "hasMaterials": bool(info.hasMaterials),
+                "boundsLo": np.array(info.boundsLo[:], np.float32), "boundsHi": np.array(info.boundsHi[:], np.float32),
+                "buildMs": info.buildMs, "totalMs": info.totalMs}
+
+    def read_built_mesh(self) -> Dict[str, np.ndarray]:
+        info = self._mesh_info
+        idx = np.zeros((info.triCount, 3), np.int32)
+        mat = np.zeros(info.triCount, np.int32)
+        pos = np.zeros((info.vertCount, 3), np.float32)
+        nrm = np.zeros((info.vertCount, 3), np.float32) if info.hasNormals else None
+        tex = np.zeros((info.vertCount, 2), np.float32) if info.hasTexcoords else None
+
+        def p(a):
+            return None if a is None or a.size == 0 else a.ctypes.data
+
+        self._check(self.L.prt_read_built_mesh(self.h, p(idx), p(mat), p(pos), p(nrm), p(tex)), "prt_read_built_mesh")
+        return {"indices": idx, "materialIds": mat, "positions": pos, "normals": nrm, "texcoords": tex}
+
+    def save_built_mesh(self, path: str):
+        self._check(self.L.prt_save_built_mesh(self.h, path.encode()), "prt_save_built_mesh")
+
     def render_batch(self, requests: Sequence[dict]) -> Dict[str, float]:
         """requests: dicts with scene (Context), camera (Camera), width, height,
         spp, maxDepth, accum (numpy (H,W,4) float32 or a device tensor)."""
@@ -384,12 +459,13 @@ class Device:
         return self.ctx.scene_bounds()
 
     def initRenderer(self, props: dict, stats: dict):
-        """props: type (diffuse | diffuseFast), maxDepth (default 6,
-        render/diffuse_integrator_single.h:35), imageSize."""
+        """props: type (diffuse | diffuseFast | diffuse2 | diffuse2Fast),
+        maxDepth (default 6, render/diffuse_integrator_single.h:35)."""
         rtype = props.get("type", "diffuse")
-        if rtype not in ("diffuse", "diffuseFast"):
+        if rtype not in ("diffuse", "diffuseFast", "diffuse2", "diffuse2Fast"):
             raise ValueError("invalid renderer type")
-        self.accumulate = rtype == "diffuse"
+        self.accumulate = rtype in ("diffuse", "diffuse2")
+        self.ctx.set_integrator("diffuse2" if rtype.startswith("diffuse2") else "diffuse")
         self.max_depth = int(props.get("maxDepth", 6))
         stats.update({k: v for k, v in self.ctx.build().items() if k in ("buildMs", "buildMprim")})
 

@@ -144,6 +144,39 @@ def read_mesh(path: str) -> Mesh:
     return Mesh(attrs[:, :3].copy(), idx, mat, names)
 
 
+def read_mesh_blob(data) -> dict:
+    """Every field of a `.mesh` blob (geometry/triangle_mesh.cpp:305-320) from
+    a path or bytes: bounds, counts, normal/texcoord flags, indices, material
+    ids, the interleaved vertex attributes and the material names."""
+    if isinstance(data, str):
+        with open(data, "rb") as f:
+            data = f.read()
+    data = bytes(data)
+    (blob_id,) = struct.unpack_from("<i", data, 0)
+    if blob_id != MESH_BLOB_ID:
+        raise ValueError("file has wrong blob ID")
+    b = np.frombuffer(data, "<f4", 6, 4)
+    tri, vert, has_n, has_t = struct.unpack_from("<ii??", data, 28)
+    stride = 3 + (3 if has_n else 0) + (2 if has_t else 0)
+    off = 38
+    idx = np.frombuffer(data, "<i4", 3 * tri, off).reshape(tri, 3)
+    off += 12 * tri
+    mat = np.frombuffer(data, "<i4", tri, off)
+    off += 4 * tri
+    attrs = np.frombuffer(data, "<f4", vert * stride, off).reshape(vert, stride)
+    off += 4 * vert * stride
+    (count,) = struct.unpack_from("<i", data, off)
+    off += 4
+    names = []
+    for _ in range(count):
+        (n,) = struct.unpack_from("<i", data, off)
+        names.append(data[off + 4:off + 4 + n].decode())
+        off += 4 + n
+    return {"lo": b[:3].copy(), "hi": b[3:].copy(), "tri": tri, "vert": vert, "has_normals": bool(has_n),
+            "has_texcoords": bool(has_t), "indices": idx.copy(), "material_ids": mat.copy(), "attrs": attrs.copy(),
+            "names": names, "size": off}
+
+
 def write_view(path: str, view: View) -> None:
     with open(path, "wb") as f:
         for _ in range(10):

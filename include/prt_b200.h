@@ -253,6 +253,70 @@ int prt_render_noalloc(prt_ctx* ctx, const prt_camera* cam, int width, int heigh
 /* Kernel launches issued by this context since creation (for accounting). */
 long long prt_launch_count(prt_ctx* ctx);
 
+/* ---- `protoray build`: OBJ -> triangle soup -> indexed .mesh ------------- */
+
+/* One soup vertex and triangle: the reference's FatVertex / FatTriangle
+ * (geometry/vertex.h:23-28, geometry/triangle.h:54-57), 32 and 100 bytes. */
+typedef struct prt_soup_vertex {
+    float pos[3];
+    float normal[3];   /* all zero: none given */
+    float tex[2];      /* all zero: none given */
+} prt_soup_vertex;
+
+typedef struct prt_soup_triangle {
+    prt_soup_vertex v[3];
+    int matId;
+} prt_soup_triangle;
+
+/* A parsed soup: triangles plus material names (geometry/triangle_soup.h:25-29). */
+typedef struct prt_soup prt_soup;
+
+/* Replaces ObjLoader::load (main/build/obj_loader.cpp:35-53): parses an OBJ
+ * file on `threads` host threads (0: all cores).  Same grammar and results as
+ * the reference: v / vn / vt / f / usemtl lines, 1-based and negative
+ * (relative) indices, faces fan-triangulated, triangles with two equal
+ * position indices dropped, material 0 named "" and "Default" added for faces
+ * before the first usemtl.  Host code only (no device is touched).  On a
+ * malformed file returns PRT_EIO and writes the reason into err. */
+int prt_soup_load_obj(const char* path, int threads, prt_soup** soup, char* err, int errlen);
+/* Counts of a soup; any output pointer may be NULL.  degenerateCount is the
+ * number of triangles the OBJ loader dropped. */
+int prt_soup_info(const prt_soup* soup, int* triCount, int* materialCount, int* degenerateCount);
+const prt_soup_triangle* prt_soup_triangles(const prt_soup* soup);
+const char* prt_soup_material_name(const prt_soup* soup, int i);
+void prt_soup_free(prt_soup* soup);
+
+/* Description of a mesh built by prt_build_mesh. */
+typedef struct prt_mesh_info {
+    int triCount;
+    int vertCount;       /* unique vertices */
+    int hasNormals;
+    int hasTexcoords;
+    int hasMaterials;    /* some matId != 0; otherwise all material ids are stored as 0 */
+    float boundsLo[3];
+    float boundsHi[3];
+    double buildMs;      /* device time of the build kernels */
+    double totalMs;      /* host soup in -> device mesh ready, copies included */
+} prt_mesh_info;
+
+/* Replaces TriangleMeshBuilder (geometry/triangle_mesh_builder.cpp:23-263) on
+ * the GPU: zero normals are replaced by the triangle's cross product when
+ * the soup has normals (:92-96), vertices equal in position, normal and
+ * texcoord are merged (:98-112), and the vertices and triangles are put in
+ * Morton order of their positions and centroids (the reference uses a median
+ * split, :143-201; both are locality orders, so the mesh holds the same
+ * vertices and triangles in a different order).  The mesh stays on the device
+ * of ctx until the next call; material names are kept with it. */
+int prt_build_mesh(prt_ctx* ctx, const prt_soup_triangle* tris, int triCount, const char* const* materialNames,
+                   int materialCount, prt_mesh_info* info);
+/* Copies the built mesh to host arrays: indices[3*triCount],
+ * materialIds[triCount], positions[3*vertCount]; normals[3*vertCount] and
+ * texcoords[2*vertCount] only when present (else pass NULL). */
+int prt_read_built_mesh(prt_ctx* ctx, int* indices, int* materialIds, float* positions, float* normals, float* texcoords);
+/* Writes the built mesh as a .mesh blob (saveBlob + operator<<,
+ * sys/blob.h:40-50, geometry/triangle_mesh.cpp:322-337). */
+int prt_save_built_mesh(prt_ctx* ctx, const char* path);
+
 #ifdef __cplusplus
 }
 #endif

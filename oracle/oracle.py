@@ -34,6 +34,13 @@ def build(with_ref: Optional[bool] = None) -> None:
     subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
 
 
+# the reference's FatTriangle (geometry/triangle.h:54-57, geometry/vertex.h:23-28):
+# three {pos, normal, tex} vertices and a material id, 100 bytes
+SOUP_VERTEX_DTYPE = np.dtype([("pos", "<f4", 3), ("normal", "<f4", 3), ("tex", "<f4", 2)])
+SOUP_DTYPE = np.dtype([("v", SOUP_VERTEX_DTYPE, 3), ("matId", "<i4")])
+assert SOUP_DTYPE.itemsize == 100
+
+
 def _f32p(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
@@ -237,6 +244,12 @@ class Reference:
             lib.ref_query_ray.restype = C.c_int
             lib.ref_query_ray.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
             lib.ref_rng.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+            lib.ref_obj_load.restype = C.c_void_p
+            lib.ref_obj_load.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p]
+            lib.ref_soup_get.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p]
+            lib.ref_soup_free.argtypes = [C.c_void_p]
+            lib.ref_build_soup.restype = C.c_double
+            lib.ref_build_soup.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_char_p]
             lib.ref_camera.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
             lib.ref_primary_rays.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
             lib.ref_cosine_sample.argtypes = [C.c_float, C.c_float, C.c_void_p]
@@ -248,6 +261,31 @@ class Reference:
 
     def open(self, path: str) -> "RefScene":
         return RefScene(self, path)
+
+    def load_obj(self, path: str):
+        """ObjLoader::load: (soup records as a SOUP_DTYPE array, material
+        names), or None when the reference loader rejects the file."""
+        n, names, nbytes = C.c_int(), C.c_int(), C.c_int()
+        h = self.lib.ref_obj_load(path.encode(), C.byref(n), C.byref(names), C.byref(nbytes))
+        if not h:
+            return None
+        try:
+            tris = np.zeros(n.value, SOUP_DTYPE)
+            buf = C.create_string_buffer(max(1, nbytes.value))
+            self.lib.ref_soup_get(h, tris.ctypes.data, buf)
+            text = buf.raw[:nbytes.value].decode()
+            return tris, text.split("\n")[:names.value]
+        finally:
+            self.lib.ref_soup_free(h)
+
+    def build_soup(self, tris: np.ndarray, names, mesh_path: str) -> float:
+        """TriangleMeshBuilder + saveBlob; returns the builder's time in ms."""
+        tris = np.ascontiguousarray(tris, SOUP_DTYPE)
+        joined = "".join(s + "\n" for s in names).encode()
+        ms = self.lib.ref_build_soup(tris.ctypes.data, len(tris), joined, len(names), mesh_path.encode())
+        if ms < 0:
+            raise RuntimeError("reference TriangleMeshBuilder failed")
+        return ms
 
     def rng(self, pass_: int, pixel: int, n: int):
         st = np.zeros(n + 1, np.uint32)

@@ -31,6 +31,9 @@
 #include "core/intersector_single.h"
 #include "core/intersector_stream.h"
 #include "image/frame_buffer.h"
+#include "main/build/obj_loader.h"
+#include "geometry/triangle_mesh_builder.h"
+#include "sys/blob.h"
 
 #include "prt_oracle.h"
 #include "cpu_bvh32.hpp"
@@ -391,6 +394,82 @@ int ref_query_ray(void* handle, const float ray[7], float* out)
     out[2] = p.x; out[3] = p.y; out[4] = p.z;
     out[5] = Ng.x; out[6] = Ng.y; out[7] = Ng.z;
     return 1;
+}
+
+// `protoray build` of the reference, split at its two seams so that each can
+// be compared on its own: ObjLoader::load (main/build/obj_loader.cpp:35-53)
+// and TriangleMeshBuilder + saveBlob (geometry/triangle_mesh_builder.cpp:23-44,
+// main/build/build.cpp:98-118).
+static_assert(sizeof(FatTriangle) == 100, "FatTriangle is 3 x 32-byte vertices + matId");
+
+struct RefSoup
+{
+    TriangleSoup soup;
+};
+
+// Parses an OBJ file.  Returns nullptr when ObjLoader::load returns false.
+void* ref_obj_load(const char* path, int* triCount, int* nameCount, int* nameBytes)
+{
+    RefSoup* h = new RefSoup;
+    ObjLoader loader;
+    if (!loader.load(path, h->soup))
+    {
+        delete h;
+        return nullptr;
+    }
+    *triCount = (int)h->soup.triangles.getSize();
+    *nameCount = (int)h->soup.materialNames.getSize();
+    size_t bytes = 0;
+    for (int i = 0; i < *nameCount; ++i) bytes += h->soup.materialNames[i].size() + 1;
+    *nameBytes = (int)bytes;
+    return h;
+}
+
+// Copies the soup out: FatTriangle records, and the material names each
+// followed by a '\n'.
+void ref_soup_get(void* handle, void* tris, char* names)
+{
+    RefSoup* h = (RefSoup*)handle;
+    std::memcpy(tris, h->soup.triangles.getData(), sizeof(FatTriangle) * (size_t)h->soup.triangles.getSize());
+    for (int i = 0; i < (int)h->soup.materialNames.getSize(); ++i)
+    {
+        const std::string& s = h->soup.materialNames[i];
+        std::memcpy(names, s.data(), s.size());
+        names += s.size();
+        *names++ = '\n';
+    }
+}
+
+void ref_soup_free(void* handle) { delete (RefSoup*)handle; }
+
+// TriangleMeshBuilder over a soup given as FatTriangle records and
+// '\n'-terminated material names; writes the .mesh blob and returns the
+// builder's own time in milliseconds (negative on failure).
+double ref_build_soup(const void* tris, int n, const char* names, int nameCount, const char* meshPath)
+{
+    try
+    {
+        TriangleSoup soup;
+        soup.triangles.alloc(n);
+        std::memcpy(soup.triangles.getData(), tris, sizeof(FatTriangle) * (size_t)n);
+        const char* p = names;
+        for (int i = 0; i < nameCount; ++i)
+        {
+            const char* e = std::strchr(p, '\n');
+            soup.materialNames.pushBack(std::string(p, e - p));
+            p = e + 1;
+        }
+        TriangleMesh mesh;
+        auto t0 = std::chrono::steady_clock::now();
+        TriangleMeshBuilder(soup, mesh);
+        auto t1 = std::chrono::steady_clock::now();
+        saveBlob(meshPath, mesh);
+        return std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    catch (const std::exception&)
+    {
+        return -1.0;
+    }
 }
 
 // ---- known-answer vectors from the reference's own code ----

@@ -15,7 +15,7 @@ HEADER = os.path.join(ROOT, "include", "prt_b200.h")
 
 def declared_symbols():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|long long|const char\*)\s+(prt_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:const\s+)?(?:int|void|long long|char|prt_\w+)\s*\*?\s+(prt_\w+)\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():

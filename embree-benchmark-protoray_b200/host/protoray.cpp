@@ -4,7 +4,7 @@
 //
 //   protoray render scene.mesh [-r diffuse|diffuseFast] [-spp N] [-size W,H]
 //       [-maxDepth D] [-dev b200] [-view K] [-benchmark PREFIX | -o PREFIX]
-//       [-warmup N] [-sppPerFrame K] [-c config] [-no-mtl] ...
+//       [-warmup N] [-sppPerFrame K] [-c config] [-checkpoint] [-runtime S] [-no-mtl] ...
 //
 // Options are `-name value` or `-name=value`; a bare argument is the scene
 // (sys/option.cpp:37-93).  Unknown options are kept as properties, as in the
@@ -265,6 +265,10 @@ int main_render(const std::vector<std::string>& args)
             values[i].push_back(st.getDouble(k, 0.0));
         }
     };
+    // -checkpoint: an image at every power-of-two spp; -runtime T: stop after T
+    // seconds (main/render/render_window.cpp:39-41, 279-304)
+    const bool checkpoint = s.props.exists("checkpoint");
+    const double runtime = s.props.getDouble("runtime", 1e300);
     int spp = 0;
     auto t0 = std::chrono::steady_clock::now();
     while (spp < maxSpp)
@@ -278,6 +282,15 @@ int main_render(const std::vector<std::string>& args)
         st.set("renderMs", frameMs);
         st.set("fps", 1000.0 / frameMs);
         if (spp > warmupSpp || !s.benchmark) record(st);
+        if (checkpoint && (spp & (spp - 1)) == 0)
+        {
+            char name[32];
+            std::snprintf(name, sizeof(name), "%06dspp", spp);
+            std::vector<uint32_t> px;
+            dev.blitFrame(px);
+            save_ppm(s.prefix + "_" + name + ".ppm", px, s.width, s.height);
+        }
+        if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= runtime) break;
     }
     double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     say("Rendered " + std::to_string(spp) + " spp in " + std::to_string(total) + " s");

@@ -77,3 +77,18 @@ def test_cli_config_file_and_default_view(tmp_path, small):
     assert r.returncode == 0, r.stderr
     assert "Default view" in r.stdout
     assert os.path.exists(str(tmp_path / "cfg.ppm"))
+
+
+def test_cli_checkpoint_images(tmp_path, small):
+    """-checkpoint writes <prefix>_<spp>spp.ppm at every power-of-two spp
+    (main/render/render_window.cpp:279-292); the last equals the final image."""
+    import scenes
+    path = scenes.write_scene(str(tmp_path), "small", *small)
+    prefix = str(tmp_path / "cp")
+    r = subprocess.run([EXE, "render", path, "-spp", "5", "-size", "32,24", "-maxDepth", "3", "-checkpoint",
+                        "-o", prefix], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    for n in (1, 2, 4):
+        assert os.path.exists(f"{prefix}_{n:06d}spp.ppm")
+    assert not os.path.exists(f"{prefix}_000003spp.ppm") and not os.path.exists(f"{prefix}_000005spp.ppm")
+    assert _read_ppm(f"{prefix}_000004spp.ppm")[2].shape == (24, 32, 3)

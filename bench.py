@@ -395,6 +395,94 @@ def run_mesh_build(prt, torch, device):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def run_kernel_tour(prt, torch, device):
+    """Launches every kernel family of the library once on a case whose inputs
+    exceed L2 where the kernel reads bulk data, for profiler captures
+    (`ncu ... python bench.py --kernel-tour`); prints one JSON line of
+    CUDA-event times.  Phases: LBVH build of 2000 level-4 icospheres (10.2M
+    triangles); 4M incoherent closest-hit and any-hit queries on the terrain;
+    one diffuse2 render (960x540, 4 spp); path-replay forward and backward
+    (small scene, 512x512, 4 spp, per-triangle albedo); a batch of 8 requests;
+    the LDR resolve of a 3840x2160 frame; the mesh builder on the terrain as a
+    soup (1.38M triangles, 138 MB)."""
+    import scenes
+    dev = f"cuda:{device}"
+    out = {}
+
+    def timed(name, fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        out[name + "_ms"] = round(a.elapsed_time(b), 3)
+
+    m, _ = scenes.spheres10m_scene()
+    c = prt.Context(device)
+    c.load_mesh(m.indices, m.positions)
+    timed("build_10m", c.build)
+    c.close()
+
+    terrain, tview = scenes.terrain_scene()
+    c = prt.Context(device)
+    c.load_mesh(terrain.indices, terrain.positions)
+    c.build()
+    n = 1 << 22
+    g = torch.Generator(device=dev).manual_seed(5)
+    lo, hi = terrain.positions.min(0), terrain.positions.max(0)
+    rays = torch.zeros((n, 8), dtype=torch.float32, device=dev)
+    for k in range(3):
+        rays[:, k] = float(lo[k]) + torch.rand(n, generator=g, device=dev) * float(hi[k] - lo[k])
+    d = torch.randn((n, 3), generator=g, device=dev)
+    rays[:, 4:7] = d / d.norm(dim=1, keepdim=True)
+    rays[:, 7] = 3.0e38
+    hits = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    occ = torch.zeros(n, dtype=torch.float32, device=dev)
+    timed("intersect_4m", lambda: c.intersect(rays, hits, n))
+    timed("occluded_4m", lambda: c.occluded(rays, occ, n))
+    c.set_integrator("diffuse2")
+    c.init_frame(960, 540)
+    c.set_view(tview, 960, 540)
+    timed("diffuse2_960x540x4", lambda: c.render(4, 5, accumulate=False))
+    c.init_frame(3840, 2160)
+    timed("resolve_ldr_4k", c.read_ldr)
+    c.close()
+
+    small, sview = scenes.small_scene()
+    c = prt.Context(device)
+    c.load_mesh(small.indices, small.positions)
+    c.set_albedo(torch.from_numpy(scenes.albedo_for(small)).to(dev))
+    c.build()
+    c.init_frame(512, 512)
+    c.set_view(sview, 512, 512)
+    gimg = torch.randn((512, 512, 3), dtype=torch.float32, device=dev)
+    d_alb = torch.zeros(small.tri_count, dtype=torch.float32, device=dev)
+    d_sky = torch.zeros(1, dtype=torch.float32, device=dev)
+    timed("replay_fwd_512x4", lambda: c.render_replay(0, 4, 5))
+    timed("replay_bwd_512x4", lambda: c.render_backward(0, 4, 5, gimg, d_alb, d_sky))
+    c.close()
+    c = prt.Context(device)   # batched requests use the constant albedo
+    c.load_mesh(small.indices, small.positions)
+    c.build()
+    reqs = []
+    for k in range(8):
+        w, h = 128 + 64 * k, 512 - 32 * k
+        reqs.append({"scene": c, "camera": prt.camera_from_view(sview, w, h), "width": w, "height": h,
+                     "spp": 1 + 3 * k, "maxDepth": 5,
+                     "accum": torch.zeros((h, w, 4), dtype=torch.float32, device=dev)})
+    timed("batch_8", lambda: c.render_batch(reqs))
+    c.close()
+
+    soup = np.zeros(terrain.tri_count, prt.SOUP_DTYPE)
+    soup["v"]["pos"] = terrain.positions[terrain.indices]
+    c = prt.Context(device)
+    timed("mesh_build_1.38m", lambda: c.build_mesh(soup, ["", "Default"]))
+    c.close()
+    print(json.dumps({"kernel_tour": out}))
+    return 0
+
+
 def main():
     global W, H, SPP
     ap = argparse.ArgumentParser()
@@ -408,12 +496,20 @@ def main():
     ap.add_argument("--width", type=int, default=W, help="smaller frames are for profiling captures only")
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--kernel-tour", action="store_true",
+                    help="launch every kernel family once on small cases (for profiler captures) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel_tour:
+        import torch
+        sys.path.insert(0, PKG)
+        import prt
+        torch.cuda.set_device(0)
+        return run_kernel_tour(prt, torch, 0)
     W, H, SPP = args.width, args.height, args.spp
 
     rank, world, local = dist_env()

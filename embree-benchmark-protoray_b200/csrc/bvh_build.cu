@@ -117,17 +117,25 @@ __global__ void k_reduce_bounds(const float* __restrict__ partial, int nblocks, 
 
 // --- 2. Morton codes -------------------------------------------------------
 
+// Cells of the Morton grid: per-axis normalisation (0) stretches a flat scene's
+// thin axis to the full 10 bits, so high tree levels split along it; cubic
+// cells (1) normalise every axis by the largest extent.
+#ifndef PRT_MORTON_CUBE
+#define PRT_MORTON_CUBE 0
+#endif
+
 __global__ void k_morton(const float* __restrict__ triBox, int nt, const float* __restrict__ cb, uint32_t* __restrict__ keys,
                          uint32_t* __restrict__ vals)
 {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nt) return;
     uint32_t code = 0;
+    const float extMax = fmaxf(cb[3] - cb[0], fmaxf(cb[4] - cb[1], cb[5] - cb[2]));
 #pragma unroll
     for (int k = 0; k < 3; ++k)
     {
         float c = 0.5f * (triBox[6 * (size_t)p + k] + triBox[6 * (size_t)p + 3 + k]);
-        float ext = cb[3 + k] - cb[k];
+        float ext = PRT_MORTON_CUBE ? extMax : cb[3 + k] - cb[k];
         float u = ext > 0.f ? (c - cb[k]) / ext : 0.f;
         uint32_t q = (uint32_t)fminf(fmaxf(u * 1024.0f, 0.0f), 1023.0f);
         code |= expand10(q) << k;

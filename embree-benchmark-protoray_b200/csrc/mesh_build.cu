@@ -126,13 +126,21 @@ __global__ void __launch_bounds__(256) k_soup_scan(const float* __restrict__ sou
     }
 }
 
-__global__ void k_bounds_final(const float* __restrict__ partial, int nblocks, float* __restrict__ out)
+// One warp per bound component (6 warps): strided reads of the block partials, then a shuffle reduction.
+__global__ void __launch_bounds__(192) k_bounds_final(const float* __restrict__ partial, int nblocks,
+                                                      float* __restrict__ out)
 {
-    const int k = threadIdx.x;
-    if (k >= 6) return;
-    float v = k < 3 ? FLT_MAX : -FLT_MAX;
-    for (int b = 0; b < nblocks; ++b) v = k < 3 ? fminf(v, partial[6 * b + k]) : fmaxf(v, partial[6 * b + k]);
-    out[k] = v;
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool isMin = k < 3;
+    float v = isMin ? FLT_MAX : -FLT_MAX;
+    for (int b = lane; b < nblocks; b += 32) v = isMin ? fminf(v, partial[6 * b + k]) : fmaxf(v, partial[6 * b + k]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        const float o = __shfl_xor_sync(0xffffffffu, v, off);
+        v = isMin ? fminf(v, o) : fmaxf(v, o);
+    }
+    if (lane == 0) out[k] = v;
 }
 
 // 2. corner records and triangle keys --------------------------------------------
@@ -401,7 +409,7 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
     MB_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned) * 2, stream));
     MB_CHECK(cudaEventRecord(ev0, stream));
     k_soup_scan<<<scanBlocks, 256, 0, stream>>>(soup, n, small, partial);
-    k_bounds_final<<<1, 32, 0, stream>>>(partial, scanBlocks, bounds);
+    k_bounds_final<<<1, 192, 0, stream>>>(partial, scanBlocks, bounds);
     launches += 2;
     if (n > 0)
     {

@@ -86,6 +86,12 @@ struct prt_ctx
     cudaEvent_t forkEv = nullptr;
     cudaEvent_t joinEv[kMaxChains] = {};
 
+    // work counters of prt_intersect / prt_occluded calls: a ring, so that
+    // calls issued on different streams do not share one
+    static constexpr int kIsectSlots = 64;
+    int* dIsect = nullptr;
+    int isectNext = 0;
+
     // query scratch
     RayRec* dRay = nullptr;
     HitRec* dHit = nullptr;
@@ -602,6 +608,16 @@ int load_mesh_file(prt_ctx* ctx, const char* path, float outLo[3], float outHi[3
     return PRT_OK;
 }
 
+// A zeroed work counter for one prt_intersect / prt_occluded launch on stream s.
+int isect_counter(prt_ctx* ctx, cudaStream_t s, int** out)
+{
+    if (!ctx->dIsect) CK(dev_malloc(&ctx->dIsect, sizeof(int) * prt_ctx::kIsectSlots));
+    int* c = ctx->dIsect + (ctx->isectNext++ % prt_ctx::kIsectSlots);
+    CK(cudaMemsetAsync(c, 0, sizeof(int), s));
+    *out = c;
+    return PRT_OK;
+}
+
 } // namespace
 
 prt_ctx::~prt_ctx()
@@ -629,6 +645,7 @@ prt_ctx::~prt_ctx()
         if (joinEv[c]) cudaEventDestroy(joinEv[c]);
     }
     if (forkEv) cudaEventDestroy(forkEv);
+    cudaFree(dIsect);
     cudaFree(dRay);
     cudaFree(dHit);
     cudaFree(dPNg);
@@ -1065,7 +1082,10 @@ int prt_intersect(prt_ctx* ctx, const prt_ray* rays, prt_hit* hits, int n, void*
         return fail(ctx, PRT_EINVAL, "prt_intersect takes device pointers");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    ctx->launches += launch_intersect(scene_dev(ctx), (const RayRec*)rays, (HitRec*)hits, n, false, nullptr, s);
+    int* fetch = nullptr;
+    st = isect_counter(ctx, s, &fetch);
+    if (st != PRT_OK) return st;
+    ctx->launches += launch_intersect(scene_dev(ctx), (const RayRec*)rays, (HitRec*)hits, n, false, nullptr, fetch, ctx->numSMs, s);
     CK(cudaGetLastError());
     if (!stream) CK(cudaStreamSynchronize(ctx->stream));
     return PRT_OK;
@@ -1080,7 +1100,10 @@ int prt_occluded(prt_ctx* ctx, const prt_ray* rays, float* out, int n, void* str
         return fail(ctx, PRT_EINVAL, "prt_occluded takes device pointers");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    ctx->launches += launch_intersect(scene_dev(ctx), (const RayRec*)rays, nullptr, n, true, out, s);
+    int* fetch = nullptr;
+    st = isect_counter(ctx, s, &fetch);
+    if (st != PRT_OK) return st;
+    ctx->launches += launch_intersect(scene_dev(ctx), (const RayRec*)rays, nullptr, n, true, out, fetch, ctx->numSMs, s);
     CK(cudaGetLastError());
     if (!stream) CK(cudaStreamSynchronize(ctx->stream));
     return PRT_OK;

@@ -172,8 +172,9 @@ struct LaunchCfg
 
 // Kernel launchers (render.cu).  Each returns the number of launches issued.
 int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s);
+// fetch: a zeroed work counter on the device, used by this launch only
 int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n, bool anyHit, float* anyOut,
-                     cudaStream_t s);
+                     int* fetch, int numSMs, cudaStream_t s);
 int launch_resolve_ldr(const float4* accum, uint32_t* out, int n, cudaStream_t s);
 int launch_advance_pass(int* passBase, int spp, cudaStream_t s);
 int launch_query(const SceneDev& sc, const RayRec* ray, HitRec* hit, float* pNg, cudaStream_t s);

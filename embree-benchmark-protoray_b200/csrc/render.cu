@@ -429,34 +429,75 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
     if (lane == 0 && shadowRays) atomicAdd(a.rays, shadowRays);
 }
 
+// The IntersectorStreamCuda seam (core/intersector_stream_cuda.h:32-33):
+// closest or any hit for n ray records.  Persistent warps with the same
+// dynamic per-lane refill as k_bounce: a lane whose query is complete writes
+// its hit record, and once kRefillMin lanes of the warp are free they claim
+// the next rays from the call's work counter, so incoherent queries of very
+// different lengths keep the warp's lanes busy.
 template <bool kAnyHit>
-__global__ void __launch_bounds__(128) k_intersect(SceneDev sc, const RayRec* __restrict__ rays, HitRec* __restrict__ hits,
-                                                   float* __restrict__ anyOut, int n)
+__global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneDev sc, const RayRec* __restrict__ rays,
+                                                                         HitRec* __restrict__ hits,
+                                                                         float* __restrict__ anyOut, int n, int* fetch)
 {
     extern __shared__ uint2 s_stack[];
     TravStack st;
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned ltMask = (1u << lane) - 1u;
+    bool has = false, exhausted = false;
+    int idx = 0;
+    float tnear = 0.f;
+    TravRay r;
+    TravState ts;
+    ts.done = true;
+    for (;;)
     {
-        const float4* rp = reinterpret_cast<const float4*>(rays + i);
-        float4 a = __ldg(rp), b = __ldg(rp + 1);
-        TravRay r;
-        trav_setup(r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
-        float t, u, v;
-        int prim;
-        int ti = traverse<kAnyHit>(sc, r, a.w, b.w, st, t, prim, u, v);
-        if (kAnyHit)
+        unsigned idle = __ballot_sync(FULL, !has);
+        if (!exhausted && (__popc(idle) >= kRefillMin || idle == FULL))
         {
-            anyOut[i] = ti >= 0 ? t : -1.0f;
+            int cnt = __popc(idle);
+            int base = 0;
+            if (lane == 0) base = atomicAdd(fetch, cnt);
+            base = __shfl_sync(FULL, base, 0);
+            if (base + cnt >= n) exhausted = true;
+            int i = base + __popc(idle & ltMask);
+            if (!has && i < n)
+            {
+                const float4* rp = reinterpret_cast<const float4*>(rays + i);
+                float4 a = __ldcs(rp), b = __ldcs(rp + 1);
+                trav_setup(r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+                trav_init(ts, sc, b.w, st);
+                tnear = a.w;
+                idx = i;
+                has = true;
+            }
         }
-        else
+        if (__ballot_sync(FULL, has) == 0)
         {
-            HitRec h;
-            if (ti >= 0) { h.t = t; h.primId = prim; h.u = u; h.v = v; }
-            else { h.t = -1.0f; h.primId = -1; h.u = 0.f; h.v = 0.f; }
-            reinterpret_cast<float4*>(hits)[i] = make_float4(h.t, __int_as_float(h.primId), h.u, h.v);
+            if (exhausted) break;
+            continue;
+        }
+        for (;;)
+        {
+            if (has && !ts.done) trav_step<kAnyHit>(ts, sc, r, tnear, st);
+            unsigned running = __ballot_sync(FULL, has && !ts.done);
+            if (running == 0) break;
+            if (!exhausted && 32 - __popc(running) >= kRefillMin) break;
+        }
+        if (has && ts.done)
+        {
+            const bool hit = ts.triHit >= 0;
+            if (kAnyHit)
+                __stcs(anyOut + idx, hit ? ts.tHit : -1.0f);
+            else
+                __stcs(reinterpret_cast<float4*>(hits) + idx,
+                       hit ? make_float4(ts.tHit, __int_as_float(ts.primHit), ts.uHit, ts.vHit)
+                           : make_float4(-1.0f, __int_as_float(-1), 0.f, 0.f));
+            has = false;
         }
     }
 }
@@ -877,15 +918,19 @@ int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int
 }
 
 int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n, bool anyHit, float* anyOut,
-                     cudaStream_t s)
+                     int* fetch, int numSMs, cudaStream_t s)
 {
     if (n <= 0) return 0;
-    int block = 128;
-    int grid = (n + block - 1) / block;
-    if (grid > 148 * 16) grid = 148 * 16;
-    size_t shmem = sizeof(uint2) * kShared * block;
-    if (anyHit) k_intersect<true><<<grid, block, shmem, s>>>(sc, rays, hits, anyOut, n);
-    else k_intersect<false><<<grid, block, shmem, s>>>(sc, rays, hits, anyOut, n);
+    const int block = 128;
+    const size_t shmem = sizeof(uint2) * kShared * block;
+    LaunchCfg cfg;
+    auto go = [&](auto kernel) {
+        // no more warps than rays: 32 rays per warp
+        int grid = std::min(grid_for(kernel, block, shmem, numSMs, cfg), (n + block - 1) / block);
+        kernel<<<grid, block, shmem, s>>>(sc, rays, hits, anyOut, n, fetch);
+    };
+    if (anyHit) go(k_intersect<true>);
+    else go(k_intersect<false>);
     return 1;
 }
 

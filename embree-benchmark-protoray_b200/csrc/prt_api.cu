@@ -187,13 +187,23 @@ CameraDev camera_dev(const prt_camera& c, int W, int H)
     return d;
 }
 
-__global__ void k_check_indices(const int* idx, long long n3, int nv, int* bad)
+// Counts indices outside [0, nv): 16-byte loads over the bulk of the array
+// (cudaMalloc memory is 256-byte aligned), scalar loads for the tail.
+__global__ void k_check_indices(const int* __restrict__ idx, long long n3, int nv, int* bad)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long n4 = n3 >> 2;
+    const unsigned unv = (unsigned)nv;
+    int count = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride)
     {
-        int v = idx[i];
-        if (v < 0 || v >= nv) atomicAdd(bad, 1);
+        int4 v = __ldcs(reinterpret_cast<const int4*>(idx) + i);
+        count += ((unsigned)v.x >= unv) + ((unsigned)v.y >= unv) + ((unsigned)v.z >= unv) + ((unsigned)v.w >= unv);
     }
+    for (long long i = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += stride)
+        count += (unsigned)idx[i] >= unv;
+    count = __reduce_add_sync(0xffffffffu, count);
+    if ((threadIdx.x & 31) == 0 && count) atomicAdd(bad, count);
 }
 
 int ensure_queues(prt_ctx* ctx, long long paths, bool withThr, int chains = 1, bool withL = false)
@@ -400,10 +410,25 @@ __global__ void k_deinterleave(const float* __restrict__ attrs, int stride, int 
     }
 }
 
+// Per-warp position bounds: each thread reads 4 vertices as three 16-byte
+// loads (48 bytes), the last nv % 4 vertices with scalar loads.
 __global__ void k_bounds_partial(const float* __restrict__ pos, int nv, float* __restrict__ partial)
 {
     float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    const int quads = nv >> 2;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x)
+    {
+        const float4* p4 = reinterpret_cast<const float4*>(pos) + 3 * (size_t)q;
+        const float4 a = __ldcs(p4), b = __ldcs(p4 + 1), c = __ldcs(p4 + 2);
+        const float f[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int j = 0; j < 12; ++j)
+        {
+            lo[j % 3] = fminf(lo[j % 3], f[j]);
+            hi[j % 3] = fmaxf(hi[j % 3], f[j]);
+        }
+    }
+    for (int v = 4 * quads + blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
         for (int k = 0; k < 3; ++k)
         {
             float x = pos[3 * (size_t)v + k];
@@ -438,14 +463,14 @@ int install_mesh(prt_ctx* ctx, int* dIdx, float* dPos, int nt, int nv, const flo
     };
     int* dBad = nullptr;
     float* dPart = nullptr;
-    const int blocks = 128, threads = 256, warps = blocks * threads / 32;
+    const int blocks = 4 * ctx->numSMs, threads = 256, warps = blocks * threads / 32;
     cudaError_t e = dev_malloc(&dBad, sizeof(int));
     if (e == cudaSuccess) e = dev_malloc(&dPart, sizeof(float) * 6 * warps);
     if (e == cudaSuccess) e = cudaMemsetAsync(dBad, 0, sizeof(int), ctx->stream);
     if (e == cudaSuccess && nt)
     {
         // every index must name a vertex: the kernels gather positions unchecked
-        k_check_indices<<<256, 256, 0, ctx->stream>>>(dIdx, 3LL * nt, nv, dBad);
+        k_check_indices<<<blocks, threads, 0, ctx->stream>>>(dIdx, 3LL * nt, nv, dBad);
         ctx->launches++;
     }
     if (e == cudaSuccess && nv && !lo)

@@ -575,6 +575,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         }
         out.nodeCount = hostCounters[0];
         out.triCount = hostCounters[1];
+        out.leafMax = a.leafMax;
         out.levels = levels;
         if (out.triCount != n)
         {

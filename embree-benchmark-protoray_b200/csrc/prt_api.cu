@@ -166,6 +166,7 @@ SceneDev scene_dev(const prt_ctx* ctx)
     s.albedo = ctx->dAlbedo;
     s.triCount = ctx->nt;
     s.hasRoot = ctx->bvh.nodeCount > 0 ? 1 : 0;
+    s.leafTris = ctx->bvh.leafMax;
     return s;
 }
 

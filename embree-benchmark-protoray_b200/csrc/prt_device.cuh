@@ -192,6 +192,7 @@ struct SceneDev
     const float* albedo;   // per original triangle id, or nullptr (constant 0.8)
     int triCount;
     int hasRoot;           // 0 for an empty scene
+    int leafTris;          // most triangles in one leaf (the build's leaf size)
 };
 
 // Per-ray constants for traversal.
@@ -310,6 +311,24 @@ __device__ __forceinline__ float byte_unit(uint32_t x, int j)
 #define PRT_FAST_DECODE 1
 #endif
 
+// Paired FP32 FMA of sm_100 (fma.rn.f32x2): two child planes per instruction.
+#ifndef PRT_FFMA2
+#define PRT_FFMA2 0
+#endif
+
+// {a0, a1} * {s, s} + {o, o}, each lane rounded once, as two fmaf calls would.
+__device__ __forceinline__ float2 ffma2(float a0, float a1, float s, float o)
+{
+    unsigned long long a, b, c, d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(a) : "f"(a0), "f"(a1));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(b) : "f"(s));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(c) : "f"(o));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(d));
+    return r;
+}
+
 // Intersection of the ray with the 8 child boxes of a node.  Returns the hit
 // mask: bits 24..31 internal children (traversal order), bits 0..23 triangles
 // relative to the node's triangle base.
@@ -352,6 +371,26 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
         uint32_t inner4 = ((m4 & (m4 << 1)) & 0x10101010u) >> 4;           // 1 per internal byte
         uint32_t index4 = (m4 ^ (octinv4 & (inner4 * 0xffu))) & 0x1f1f1f1fu;
         uint32_t bits4 = (m4 >> 5) & 0x07070707u;
+        if (PRT_FFMA2 && PRT_FAST_DECODE)
+        {
+#pragma unroll
+            for (int j = 0; j < 4; j += 2)
+            {
+                const float2 nX = ffma2(byte_unit(nearX, j), byte_unit(nearX, j + 1), aix, aox);
+                const float2 nY = ffma2(byte_unit(nearY, j), byte_unit(nearY, j + 1), aiy, aoy);
+                const float2 nZ = ffma2(byte_unit(nearZ, j), byte_unit(nearZ, j + 1), aiz, aoz);
+                const float2 fX = ffma2(byte_unit(farX, j), byte_unit(farX, j + 1), aix, aox);
+                const float2 fY = ffma2(byte_unit(farY, j), byte_unit(farY, j + 1), aiy, aoy);
+                const float2 fZ = ffma2(byte_unit(farZ, j), byte_unit(farZ, j + 1), aiz, aoz);
+                const float t0a = fmax3(nX.x, nY.x, fmaxf(nZ.x, tnear)), t1a = fmin3(fX.x, fY.x, fminf(fZ.x, tfarp));
+                const float t0b = fmax3(nX.y, nY.y, fmaxf(nZ.y, tnear)), t1b = fmin3(fX.y, fY.y, fminf(fZ.y, tfarp));
+                if (t0a <= t1a * 1.0000008f)
+                    hits |= ((bits4 >> (8 * j)) & 0xffu) << ((index4 >> (8 * j)) & 0xffu);
+                if (t0b <= t1b * 1.0000008f)
+                    hits |= ((bits4 >> (8 * j + 8)) & 0xffu) << ((index4 >> (8 * j + 8)) & 0xffu);
+            }
+            continue;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
@@ -381,6 +420,67 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
         }
     }
     return hits;
+}
+
+// Node test for trees with one-triangle leaves (the default build): every
+// non-empty child owns exactly one hit bit, so the test sets bit `slot` of an
+// 8-bit mask per child hit instead of assembling the general mask from the
+// meta bytes.  Non-empty slots have bit 5 of their meta byte set (0x20 for an
+// internal child, a unary count of 1 for a leaf); leaf triangles are stored in
+// slot order, so the triangle of leaf slot j is triBase + popc(leafMask below j).
+// Returns internal hits at bits 24 + (slot ^ octinv) as node_hits does, leaf
+// hits as slot bits 0..7, and the node's leaf-slot mask in leafMask.
+__device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q, float tnear, float tfar,
+                                               uint32_t& leafMask)
+{
+    float px = __uint_as_float(q[0].x), py = __uint_as_float(q[0].y), pz = __uint_as_float(q[0].z);
+    uint32_t e = q[0].w;
+    float sx = __uint_as_float(((e & 0xffu) + 15u) << 23);
+    float sy = __uint_as_float((((e >> 8) & 0xffu) + 15u) << 23);
+    float sz = __uint_as_float((((e >> 16) & 0xffu) + 15u) << 23);
+    float aix = sx * r.inv.x, aiy = sy * r.inv.y, aiz = sz * r.inv.z;
+    float aox = (px - r.org.x) * r.inv.x - aix, aoy = (py - r.org.y) * r.inv.y - aiy, aoz = (pz - r.org.z) * r.inv.z - aiz;
+    bool nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
+    uint32_t loX[2] = {q[2].x, q[2].y}, loY[2] = {q[2].z, q[2].w}, loZ[2] = {q[3].x, q[3].y};
+    uint32_t hiX[2] = {q[3].z, q[3].w}, hiY[2] = {q[4].x, q[4].y}, hiZ[2] = {q[4].z, q[4].w};
+    const float tfarp = tfar * 1.0000004f;
+    uint32_t c8 = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+    {
+        uint32_t nearX = nx ? hiX[h] : loX[h], farX = nx ? loX[h] : hiX[h];
+        uint32_t nearY = ny ? hiY[h] : loY[h], farY = ny ? loY[h] : hiY[h];
+        uint32_t nearZ = nz ? hiZ[h] : loZ[h], farZ = nz ? loZ[h] : hiZ[h];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            float tnx = fmaf(byte_unit(nearX, j), aix, aox);
+            float tny = fmaf(byte_unit(nearY, j), aiy, aoy);
+            float tnz = fmaf(byte_unit(nearZ, j), aiz, aoz);
+            float tfx = fmaf(byte_unit(farX, j), aix, aox);
+            float tfy = fmaf(byte_unit(farY, j), aiy, aoy);
+            float tfz = fmaf(byte_unit(farZ, j), aiz, aoz);
+            float t0 = fmax3(tnx, tny, fmaxf(tnz, tnear));
+            float t1 = fmin3(tfx, tfy, fminf(tfz, tfarp));
+            if (t0 <= t1 * 1.0000008f) c8 |= 1u << (4 * h + j);
+        }
+    }
+    // bit 5 of each meta byte -> one bit per slot (multiply gathers bytes 0..3 into bits 24..27)
+    const uint32_t ne = ((((q[1].z >> 5) & 0x01010101u) * 0x01020408u) >> 24) |
+                        (((((q[1].w >> 5) & 0x01010101u) * 0x01020408u) >> 24) << 4);
+    c8 &= ne;
+    const uint32_t imask = q[0].w >> 24;
+    leafMask = ne & ~imask;
+    // internal hits: bit slot -> bit slot ^ octinv (three conditional swaps)
+    uint32_t in8 = c8 & imask;
+    const uint32_t o = r.octinv;
+    uint32_t sw = ((in8 & 0x55u) << 1) | ((in8 >> 1) & 0x55u);
+    in8 = (o & 1u) ? sw : in8;
+    sw = ((in8 & 0x33u) << 2) | ((in8 >> 2) & 0x33u);
+    in8 = (o & 2u) ? sw : in8;
+    sw = ((in8 & 0x0fu) << 4) | ((in8 >> 4) & 0x0fu);
+    in8 = (o & 4u) ? sw : in8;
+    return (in8 << 24) | (c8 & leafMask);
 }
 
 // Traversal stack: the first kShared entries of each thread live in shared
@@ -539,6 +639,181 @@ __device__ __forceinline__ void trav_step(TravState& s, const SceneDev& sc, cons
         ng = st.pop();   // a node group, or a postponed triangle group (bits 0..23 only)
     }
     s.ng = ng;
+}
+
+// ---- deferred triangle tests -------------------------------------------------
+//
+// With one-triangle leaves a node visit finds a triangle for only a few lanes
+// of a warp, so testing triangles in the visiting lane runs the test with ~3 of
+// 32 lanes.  In the deferred mode a node visit only queues its hit triangles
+// (leaf-order index + owner lane) in a per-warp ring in shared memory; once 32
+// are pending, the whole warp tests them, one per lane, with the owner's ray
+// fetched by shuffles, and the owners' closest hits are merged with one 64-bit
+// shared-memory atomicMin on (t bits, primitive id): positive floats order as
+// their bit patterns and the id breaks exact ties the way tri_test does.  Node
+// culling uses the owner's tHit as of the last merge, which can only be larger
+// than the final one, so no node that holds the closest hit is skipped.
+#ifndef PRT_DEFER_TRIS
+#define PRT_DEFER_TRIS 1
+#endif
+#ifndef PRT_DEFER_FLUSH
+#define PRT_DEFER_FLUSH 32
+#endif
+
+constexpr uint32_t kTriQCap = 512;   // > 31 pending + 8 triangles x 32 lanes from one step
+constexpr uint32_t kTriQMask = kTriQCap - 1;
+
+struct TriQueue
+{
+    unsigned long long key[32];   // per owner lane: (t bits << 32) | primitive id
+    uint32_t tri[kTriQCap];       // leaf-order triangle index
+    float u[32], v[32];
+    int ti[32];
+    uint8_t own[kTriQCap];        // owner lane
+};
+
+__device__ __forceinline__ unsigned long long hit_key(float t, int prim)
+{
+    return ((unsigned long long)__float_as_uint(t) << 32) | (uint32_t)prim;
+}
+
+// One node visit of the deferred mode: returns the node's hit triangles
+// (tbase + set bits of tbits) instead of testing them.
+#ifndef PRT_LEAF1_HITS
+#define PRT_LEAF1_HITS 1
+#endif
+
+// tbits: the hit leaf slots (PRT_LEAF1_HITS) with the node's leaf-slot mask in
+// leafMask, or triangle offset bits with leafMask = 0.
+__device__ __forceinline__ void trav_visit(TravState& s, const SceneDev& sc, const TravRay& r, float tnear, TravStack& st,
+                                           uint32_t& tbase, uint32_t& tbits, uint32_t& leafMask,
+                                           uint32_t* nodeVisits = nullptr)
+{
+    uint2 ng = s.ng;
+    uint32_t b = 31u - __clz(ng.y & 0xff000000u);
+    ng.y &= ~(1u << b);
+    uint32_t slot = (b - 24u) ^ r.octinv;
+    uint32_t rel = __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
+    uint32_t nodeIdx = ng.x + rel;
+    if (ng.y & 0xff000000u) st.push(ng);
+    const uint4* qp = reinterpret_cast<const uint4*>(sc.nodes + nodeIdx);
+    uint4 q[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
+    uint32_t hits;
+    if (PRT_LEAF1_HITS)
+    {
+        hits = node_hits1(r, q, tnear, s.tHit, leafMask);
+    }
+    else
+    {
+        hits = node_hits(r, q, tnear, s.tHit);
+        leafMask = 0;
+    }
+    if (nodeVisits) ++*nodeVisits;
+    ng = make_uint2(q[1].x, (hits & 0xff000000u) | (q[0].w >> 24));
+    tbits = hits & 0x00ffffffu;
+    tbase = q[1].y;
+    if (!(ng.y & 0xff000000u))
+    {
+        if (st.sp == 0)
+        {
+            s.done = true;
+            s.ng = ng;
+            return;
+        }
+        ng = st.pop();
+    }
+    s.ng = ng;
+}
+
+// Warp-collective: appends every lane's triangles to the ring at tail
+// (leafMask != 0: tbits are leaf slots, see trav_visit).
+__device__ __forceinline__ void triq_push(TriQueue& q, uint32_t& tail, uint32_t tbase, uint32_t tbits, uint32_t leafMask,
+                                          unsigned lane)
+{
+    const unsigned FULL = 0xffffffffu;
+    const uint32_t n = __popc(tbits);
+    uint32_t x = n;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync(FULL, x, off);
+        if ((int)lane >= off) x += y;
+    }
+    uint32_t pos = tail + x - n;
+    while (tbits)
+    {
+        const uint32_t bit = __ffs(tbits) - 1u;
+        tbits &= tbits - 1u;
+        q.tri[pos & kTriQMask] = tbase + (leafMask ? __popc(leafMask & ((1u << bit) - 1u)) : bit);
+        q.own[pos & kTriQMask] = (uint8_t)lane;
+        ++pos;
+    }
+    tail += __shfl_sync(FULL, x, 31);
+}
+
+// Warp-collective: tests the m (<= 32) oldest queued triangles, one per lane,
+// and merges each owner's closest hit into its traversal state.
+__device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t m, const SceneDev& sc, const TravRay& r,
+                                           float tnear, TravState& ts, unsigned lane, uint32_t* triTests = nullptr)
+{
+    const unsigned FULL = 0xffffffffu;
+    const bool act = lane < m;
+    uint32_t tri = 0;
+    int own = 0;
+    if (act)
+    {
+        tri = q.tri[(head + lane) & kTriQMask];
+        own = q.own[(head + lane) & kTriQMask];
+    }
+    head += m;
+    TravRay o;
+    o.org.x = __shfl_sync(FULL, r.org.x, own);
+    o.org.y = __shfl_sync(FULL, r.org.y, own);
+    o.org.z = __shfl_sync(FULL, r.org.z, own);
+    o.Sx = __shfl_sync(FULL, r.Sx, own);
+    o.Sy = __shfl_sync(FULL, r.Sy, own);
+    o.Sz = __shfl_sync(FULL, r.Sz, own);
+    const int kp = __shfl_sync(FULL, r.kx | (r.ky << 2) | (r.kz << 4), own);
+    o.kx = kp & 3;
+    o.ky = (kp >> 2) & 3;
+    o.kz = kp >> 4;
+    const float tb = __shfl_sync(FULL, ts.tHit, own);
+    const int bp = __shfl_sync(FULL, ts.primHit, own);
+    const unsigned long long mine = hit_key(ts.tHit, ts.primHit);
+    q.key[lane] = mine;
+    __syncwarp();
+    bool hit = false;
+    float t = 0.f, u = 0.f, v = 0.f;
+    int prim = 0;
+    if (act)
+    {
+        const float4* tp = reinterpret_cast<const float4*>(sc.tris + tri);
+        const float4 a = __ldg(tp), bq = __ldg(tp + 1), c = __ldg(tp + 2);
+        prim = __float_as_int(a.w);
+        if (triTests) ++*triTests;
+        hit = tri_test(o, f3(a.x, a.y, a.z), f3(bq.x, bq.y, bq.z), f3(c.x, c.y, c.z), tnear, tb, prim, bp, t, u, v);
+        if (hit) atomicMin(&q.key[own], hit_key(t, prim));
+    }
+    __syncwarp();
+    if (hit && q.key[own] == hit_key(t, prim))
+    {
+        q.u[own] = u;
+        q.v[own] = v;
+        q.ti[own] = (int)tri;
+    }
+    __syncwarp();
+    const unsigned long long k = q.key[lane];
+    if (k != mine)
+    {
+        ts.tHit = __uint_as_float((uint32_t)(k >> 32));
+        ts.primHit = (int)(uint32_t)k;
+        ts.uHit = q.u[lane];
+        ts.vHit = q.v[lane];
+        ts.triHit = q.ti[lane];
+    }
+    __syncwarp();
 }
 
 // Closest hit (anyHit = false) or any hit (anyHit = true) over (tnear, tfar].

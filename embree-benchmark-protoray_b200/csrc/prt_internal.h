@@ -48,6 +48,7 @@ struct Bvh8Device
     int nodeCount = 0;
     int triCount = 0;
     int levels = 0;
+    int leafMax = 1;   // most triangles per leaf
 
     void release()
     {

@@ -90,6 +90,8 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
+    // this warp's triangle queue, after the block's stack columns
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -181,6 +183,41 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
             continue;
         }
         // --- traverse until the warp has enough idle lanes ------------------
+        if (PRT_DEFER_TRIS && a.scene.leafTris == 1)
+        {
+            // node visits queue their triangles (at most 8 per lane and step
+            // with one-triangle leaves, which the ring's capacity assumes); the warp tests them 32 at a
+            // time, and every pending test is done before any lane shades
+            uint32_t qHead = 0, qTail = 0;
+            for (;;)
+            {
+                uint32_t tbase = 0, tbits = 0, lmask = 0;
+                if (PRT_COUNTERS)
+                {
+                    cLaneSteps += __popc(__ballot_sync(FULL, has && !ts.done));
+                    cSteps += 1;
+                }
+                if (has && !ts.done)
+                    trav_visit(ts, a.scene, r, 0.0f, st, tbase, tbits, lmask, PRT_COUNTERS ? &cNodes : nullptr);
+                if (__any_sync(FULL, tbits != 0)) triq_push(*tq, qTail, tbase, tbits, lmask, lane);
+                while (qTail - qHead >= (uint32_t)PRT_DEFER_FLUSH)
+                {
+                    triq_flush(*tq, qHead, min(32u, qTail - qHead), a.scene, r, 0.0f, ts, lane,
+                               PRT_COUNTERS ? &cTris : nullptr);
+                    if (PRT_COUNTERS) cTriIters += 1;
+                }
+                unsigned running = __ballot_sync(FULL, has && !ts.done);
+                if (running == 0) break;
+                if (!exhausted && 32 - __popc(running) >= kRefillMin) break;
+            }
+            while (qTail != qHead)
+            {
+                triq_flush(*tq, qHead, min(32u, qTail - qHead), a.scene, r, 0.0f, ts, lane,
+                           PRT_COUNTERS ? &cTris : nullptr);
+                if (PRT_COUNTERS) cTriIters += 1;
+            }
+        }
+        else
         for (;;)
         {
             if (PRT_COUNTERS)
@@ -873,6 +910,8 @@ int grid_for(Kernel kernel, int block, size_t shmem, int numSMs, const LaunchCfg
 int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
 {
     size_t shmem = sizeof(uint2) * kShared * cfg.block;
+    if (PRT_DEFER_TRIS && !a.Lout && a.scene.leafTris == 1)
+        shmem += sizeof(TriQueue) * (cfg.block / 32);   // k_bounce's triangle queues
     bool albedo = a.thrIn != nullptr || a.thrOut != nullptr;
     auto go = [&](auto kernel) {
         int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);

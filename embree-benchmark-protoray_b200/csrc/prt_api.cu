@@ -1201,6 +1201,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
     std::vector<float4*> tmp((size_t)n, nullptr);
     long long total = 0;
     int maxDepth = 0;
+    int leaf1 = 1;
     std::ostringstream key;
     key << "batch:" << n << ":" << ctx->cfg.block << ":" << ctx->cfg.blocksPerSM << ":" << ctx->cfg.pathsPerWave;
     for (int r = 0; r < n; ++r)
@@ -1221,6 +1222,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
         b.maxDepth = q.maxDepth;
         b.pathBegin = total;
         total += (long long)b.tilesX * b.tilesY * 64 * q.spp;
+        if (b.scene.leafTris != 1) leaf1 = 0;
         maxDepth = std::max(maxDepth, q.maxDepth);
         key << ":" << (const void*)q.scene << "," << q.width << "x" << q.height << "," << q.spp << "," << q.maxDepth
             << "," << (const void*)q.accum;
@@ -1229,7 +1231,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
                 << q.camera.imageDy[k] << "," << q.camera.basisU[k] << "," << q.camera.basisV[k];
         key << "," << q.camera.lensRadius << "," << q.camera.focalDistance;
     }
-    key << ":sky" << ctx->sky;
+    key << ":sky" << ctx->sky << ":leaf1" << leaf1;
     // device accumulation buffers (caller's device memory in place)
     bool anyTmp = false;
     for (int r = 0; r < n; ++r)
@@ -1273,6 +1275,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
         a.rays = ctx->dRays;
         a.maxDepth = maxDepth;
         a.sky = ctx->sky;
+        a.leaf1 = leaf1;
         for (long long w0 = 0; w0 < total; w0 += ppw)
         {
             a.waveBegin = w0;

@@ -754,8 +754,10 @@ __device__ __forceinline__ void triq_push(TriQueue& q, uint32_t& tail, uint32_t 
 }
 
 // Warp-collective: tests the m (<= 32) oldest queued triangles, one per lane,
-// and merges each owner's closest hit into its traversal state.
-__device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t m, const SceneDev& sc, const TravRay& r,
+// and merges each owner's closest hit into its traversal state.  The owner's
+// ray, tnear and triangle array (lanes of a batch may traverse different
+// scenes) come from the owner lane by shuffles.
+__device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t m, const TriRec* tris, const TravRay& r,
                                            float tnear, TravState& ts, unsigned lane, uint32_t* triTests = nullptr)
 {
     const unsigned FULL = 0xffffffffu;
@@ -781,6 +783,9 @@ __device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t
     o.kz = kp >> 4;
     const float tb = __shfl_sync(FULL, ts.tHit, own);
     const int bp = __shfl_sync(FULL, ts.primHit, own);
+    const float tn = __shfl_sync(FULL, tnear, own);
+    const TriRec* otris = reinterpret_cast<const TriRec*>(
+        __shfl_sync(FULL, reinterpret_cast<unsigned long long>(tris), own));
     const unsigned long long mine = hit_key(ts.tHit, ts.primHit);
     q.key[lane] = mine;
     __syncwarp();
@@ -789,11 +794,11 @@ __device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t
     int prim = 0;
     if (act)
     {
-        const float4* tp = reinterpret_cast<const float4*>(sc.tris + tri);
+        const float4* tp = reinterpret_cast<const float4*>(otris + tri);
         const float4 a = __ldg(tp), bq = __ldg(tp + 1), c = __ldg(tp + 2);
         prim = __float_as_int(a.w);
         if (triTests) ++*triTests;
-        hit = tri_test(o, f3(a.x, a.y, a.z), f3(bq.x, bq.y, bq.z), f3(c.x, c.y, c.z), tnear, tb, prim, bp, t, u, v);
+        hit = tri_test(o, f3(a.x, a.y, a.z), f3(bq.x, bq.y, bq.z), f3(c.x, c.y, c.z), tn, tb, prim, bp, t, u, v);
         if (hit) atomicMin(&q.key[own], hit_key(t, prim));
     }
     __syncwarp();
@@ -814,6 +819,47 @@ __device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t
         ts.triHit = q.ti[lane];
     }
     __syncwarp();
+}
+
+// Warp-collective closest-hit traversal with deferred triangle tests, for
+// trees with one-triangle leaves: runs node steps until no lane of the warp is
+// traversing or, when mayStop, until refillMin lanes are idle; every queued
+// test is merged before it returns.  active: this lane holds a ray.  The
+// counter pointers (node visits, triangle tests per lane; steps, running-lane
+// steps and flushes per warp) may be null.
+__device__ __forceinline__ void warp_trav_deferred(TriQueue& q, TravState& ts, const SceneDev& sc, const TravRay& r,
+                                                   float tnear, TravStack& st, bool active, bool mayStop, int refillMin,
+                                                   unsigned lane, uint32_t* cNodes = nullptr, uint32_t* cTris = nullptr,
+                                                   unsigned long long* cSteps = nullptr,
+                                                   unsigned long long* cLaneSteps = nullptr,
+                                                   unsigned long long* cFlushes = nullptr)
+{
+    const unsigned FULL = 0xffffffffu;
+    uint32_t head = 0, tail = 0;
+    for (;;)
+    {
+        uint32_t tbase = 0, tbits = 0, lmask = 0;
+        if (cSteps)
+        {
+            *cLaneSteps += __popc(__ballot_sync(FULL, active && !ts.done));
+            *cSteps += 1;
+        }
+        if (active && !ts.done) trav_visit(ts, sc, r, tnear, st, tbase, tbits, lmask, cNodes);
+        if (__any_sync(FULL, tbits != 0)) triq_push(q, tail, tbase, tbits, lmask, lane);
+        while (tail - head >= (uint32_t)PRT_DEFER_FLUSH)
+        {
+            triq_flush(q, head, min(32u, tail - head), sc.tris, r, tnear, ts, lane, cTris);
+            if (cFlushes) *cFlushes += 1;
+        }
+        const unsigned running = __ballot_sync(FULL, active && !ts.done);
+        if (running == 0) break;
+        if (mayStop && 32 - __popc(running) >= refillMin) break;
+    }
+    while (tail != head)
+    {
+        triq_flush(q, head, min(32u, tail - head), sc.tris, r, tnear, ts, lane, cTris);
+        if (cFlushes) *cFlushes += 1;
+    }
 }
 
 // Closest hit (anyHit = false) or any hit (anyHit = true) over (tnear, tfar].

@@ -161,6 +161,7 @@ struct BatchArgs
     unsigned long long* rays;
     int maxDepth;          // largest maxDepth of the batch
     float sky;
+    int leaf1;             // every request's scene has one-triangle leaves
 };
 
 struct LaunchCfg

@@ -60,6 +60,15 @@ __device__ __forceinline__ int warp_append(bool pred, int* counter)
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// Deferred triangle tests per kernel (see warp_trav_deferred): the path-replay
+// megakernel and the intersector seam have their own switches.
+#ifndef PRT_DEFER_REPLAY
+#define PRT_DEFER_REPLAY PRT_DEFER_TRIS
+#endif
+#ifndef PRT_DEFER_ISECT
+#define PRT_DEFER_ISECT PRT_DEFER_TRIS
+#endif
+
 // Lanes refill once at least this many of a warp's 32 lanes are idle
 // (persistent threads with dynamic ray fetch, Aila & Laine, HPG 2009).
 #ifndef PRT_REFILL_MIN
@@ -185,37 +194,12 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
         // --- traverse until the warp has enough idle lanes ------------------
         if (PRT_DEFER_TRIS && a.scene.leafTris == 1)
         {
-            // node visits queue their triangles (at most 8 per lane and step
-            // with one-triangle leaves, which the ring's capacity assumes); the warp tests them 32 at a
+            // node visits queue their triangles; the warp tests them 32 at a
             // time, and every pending test is done before any lane shades
-            uint32_t qHead = 0, qTail = 0;
-            for (;;)
-            {
-                uint32_t tbase = 0, tbits = 0, lmask = 0;
-                if (PRT_COUNTERS)
-                {
-                    cLaneSteps += __popc(__ballot_sync(FULL, has && !ts.done));
-                    cSteps += 1;
-                }
-                if (has && !ts.done)
-                    trav_visit(ts, a.scene, r, 0.0f, st, tbase, tbits, lmask, PRT_COUNTERS ? &cNodes : nullptr);
-                if (__any_sync(FULL, tbits != 0)) triq_push(*tq, qTail, tbase, tbits, lmask, lane);
-                while (qTail - qHead >= (uint32_t)PRT_DEFER_FLUSH)
-                {
-                    triq_flush(*tq, qHead, min(32u, qTail - qHead), a.scene, r, 0.0f, ts, lane,
-                               PRT_COUNTERS ? &cTris : nullptr);
-                    if (PRT_COUNTERS) cTriIters += 1;
-                }
-                unsigned running = __ballot_sync(FULL, has && !ts.done);
-                if (running == 0) break;
-                if (!exhausted && 32 - __popc(running) >= kRefillMin) break;
-            }
-            while (qTail != qHead)
-            {
-                triq_flush(*tq, qHead, min(32u, qTail - qHead), a.scene, r, 0.0f, ts, lane,
-                           PRT_COUNTERS ? &cTris : nullptr);
-                if (PRT_COUNTERS) cTriIters += 1;
-            }
+            warp_trav_deferred(*tq, ts, a.scene, r, 0.0f, st, has, !exhausted, kRefillMin, lane,
+                               PRT_COUNTERS ? &cNodes : nullptr, PRT_COUNTERS ? &cTris : nullptr,
+                               PRT_COUNTERS ? &cSteps : nullptr, PRT_COUNTERS ? &cLaneSteps : nullptr,
+                               PRT_COUNTERS ? &cTriIters : nullptr);
         }
         else
         for (;;)
@@ -482,6 +466,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneD
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // closest hit, leafTris == 1
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -518,6 +503,11 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneD
             if (exhausted) break;
             continue;
         }
+        if (!kAnyHit && PRT_DEFER_ISECT && sc.leafTris == 1)
+        {
+            warp_trav_deferred(*tq, ts, sc, r, tnear, st, has, !exhausted, kRefillMin, lane);
+        }
+        else
         for (;;)
         {
             if (has && !ts.done) trav_step<kAnyHit>(ts, sc, r, tnear, st);
@@ -626,6 +616,7 @@ __global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, f
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // forward, leafTris == 1
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -684,6 +675,11 @@ __global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, f
             if (exhausted) break;
             continue;
         }
+        if (PRT_DEFER_REPLAY && !kBackward && sc.leafTris == 1)
+        {
+            warp_trav_deferred(*tq, ts, sc, r, 0.0f, st, has, true, kRefillMin, lane);
+        }
+        else
         for (;;)
         {
             if (has && !ts.done) trav_step<false>(ts, sc, r, 0.0f, st);
@@ -763,6 +759,7 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
     extern __shared__ uint2 s_dyn[];
     uint2* s_stack = s_dyn;
     long long* s_begin = reinterpret_cast<long long*>(s_dyn + kShared * blockDim.x);
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_begin + a.nreq) + (threadIdx.x >> 5);   // when a.leaf1
     for (int q = threadIdx.x; q < a.nreq; q += blockDim.x) s_begin[q] = a.reqs[q].pathBegin;
     __syncthreads();
     TravStack st;
@@ -856,6 +853,11 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
             if (exhausted) break;
             continue;
         }
+        if (PRT_DEFER_TRIS && a.leaf1)
+        {
+            warp_trav_deferred(*tq, ts, a.reqs[req].scene, r, 0.0f, st, has, !exhausted, kRefillMin, lane);
+        }
+        else
         for (;;)
         {
             if (has && !ts.done) trav_step<false>(ts, a.reqs[req].scene, r, 0.0f, st);
@@ -947,6 +949,7 @@ int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs
 int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
 {
     size_t shmem = sizeof(uint2) * kShared * cfg.block + sizeof(long long) * a.nreq;
+    if (PRT_DEFER_TRIS && a.leaf1) shmem += sizeof(TriQueue) * (cfg.block / 32);
     auto go = [&](auto kernel) {
         int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);
         kernel<<<grid, cfg.block, shmem, s>>>(a, depth);
@@ -961,7 +964,8 @@ int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n
 {
     if (n <= 0) return 0;
     const int block = 128;
-    const size_t shmem = sizeof(uint2) * kShared * block;
+    size_t shmem = sizeof(uint2) * kShared * block;
+    if (!anyHit && PRT_DEFER_ISECT && sc.leafTris == 1) shmem += sizeof(TriQueue) * (block / 32);
     LaunchCfg cfg;
     auto go = [&](auto kernel) {
         // no more warps than rays: 32 rays per warp
@@ -1000,6 +1004,9 @@ int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int p
     if (total <= 0) return 0;
     const int block = 128;
     size_t shmem = sizeof(uint2) * kShared * block;
+    // the backward kernel keeps in-lane triangle tests: with its gradient table
+    // in shared memory the queues would cost it occupancy (measured 17% slower)
+    if (PRT_DEFER_REPLAY && !backward && sc.leafTris == 1) shmem += sizeof(TriQueue) * (block / 32);
     LaunchCfg cfg;
     auto go = [&](auto kernel) {
         int grid = grid_for(kernel, block, shmem, numSMs, cfg);

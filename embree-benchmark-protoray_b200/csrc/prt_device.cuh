@@ -821,18 +821,20 @@ __device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t
     __syncwarp();
 }
 
-// Warp-collective closest-hit traversal with deferred triangle tests, for
-// trees with one-triangle leaves: runs node steps until no lane of the warp is
-// traversing or, when mayStop, until refillMin lanes are idle; every queued
-// test is merged before it returns.  active: this lane holds a ray.  The
-// counter pointers (node visits, triangle tests per lane; steps, running-lane
-// steps and flushes per warp) may be null.
+// Warp-collective traversal with deferred triangle tests, for trees with
+// one-triangle leaves: runs node steps until no lane of the warp is traversing
+// or, when mayStop, until refillMin lanes are idle; every queued test is merged
+// before it returns.  active: this lane holds a ray.  anyHit: this lane's ray
+// is an occlusion query, which stops at the first merged hit (its later queued
+// tests are still merged, which can only move the hit nearer).  The counter
+// pointers (node visits, triangle tests per lane; steps, running-lane steps and
+// flushes per warp) may be null.
 __device__ __forceinline__ void warp_trav_deferred(TriQueue& q, TravState& ts, const SceneDev& sc, const TravRay& r,
                                                    float tnear, TravStack& st, bool active, bool mayStop, int refillMin,
                                                    unsigned lane, uint32_t* cNodes = nullptr, uint32_t* cTris = nullptr,
                                                    unsigned long long* cSteps = nullptr,
                                                    unsigned long long* cLaneSteps = nullptr,
-                                                   unsigned long long* cFlushes = nullptr)
+                                                   unsigned long long* cFlushes = nullptr, bool anyHit = false)
 {
     const unsigned FULL = 0xffffffffu;
     uint32_t head = 0, tail = 0;
@@ -850,6 +852,7 @@ __device__ __forceinline__ void warp_trav_deferred(TriQueue& q, TravState& ts, c
         {
             triq_flush(q, head, min(32u, tail - head), sc.tris, r, tnear, ts, lane, cTris);
             if (cFlushes) *cFlushes += 1;
+            if (anyHit && ts.triHit >= 0) ts.done = true;
         }
         const unsigned running = __ballot_sync(FULL, active && !ts.done);
         if (running == 0) break;

@@ -61,12 +61,15 @@ __device__ __forceinline__ int warp_append(bool pred, int* counter)
 }
 
 // Deferred triangle tests per kernel (see warp_trav_deferred): the path-replay
-// megakernel and the intersector seam have their own switches.
+// megakernel, the intersector seam and the diffuse2 bounce have their own switches.
 #ifndef PRT_DEFER_REPLAY
 #define PRT_DEFER_REPLAY PRT_DEFER_TRIS
 #endif
 #ifndef PRT_DEFER_ISECT
 #define PRT_DEFER_ISECT PRT_DEFER_TRIS
+#endif
+#ifndef PRT_DEFER_NEE
+#define PRT_DEFER_NEE PRT_DEFER_TRIS
 #endif
 
 // Lanes refill once at least this many of a warp's 32 lanes are idle
@@ -296,6 +299,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // leafTris == 1
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -388,6 +392,13 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
             if (exhausted) break;
             continue;
         }
+        if (PRT_DEFER_NEE && a.scene.leafTris == 1)
+        {
+            // extension rays (closest hit) and shadow rays (any hit) share the queue
+            warp_trav_deferred(*tq, ts, a.scene, r, 0.0f, st, has, true, kRefillMin, lane, nullptr, nullptr, nullptr,
+                               nullptr, nullptr, shadow);
+        }
+        else
         for (;;)
         {
             if (has && !ts.done) trav_step<false>(ts, a.scene, r, 0.0f, st, nullptr, nullptr, shadow);
@@ -912,8 +923,8 @@ int grid_for(Kernel kernel, int block, size_t shmem, int numSMs, const LaunchCfg
 int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
 {
     size_t shmem = sizeof(uint2) * kShared * cfg.block;
-    if (PRT_DEFER_TRIS && !a.Lout && a.scene.leafTris == 1)
-        shmem += sizeof(TriQueue) * (cfg.block / 32);   // k_bounce's triangle queues
+    if (a.scene.leafTris == 1 && (a.Lout ? PRT_DEFER_NEE : PRT_DEFER_TRIS))
+        shmem += sizeof(TriQueue) * (cfg.block / 32);   // the bounce kernels' triangle queues
     bool albedo = a.thrIn != nullptr || a.thrOut != nullptr;
     auto go = [&](auto kernel) {
         int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);

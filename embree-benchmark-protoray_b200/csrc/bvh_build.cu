@@ -11,9 +11,12 @@
 //   4. binary radix tree over the sorted codes (Karras, HPG 2012); equal
 //      codes are ordered by their position, so duplicates are handled
 //   5. bottom-up bounds refit (second child to arrive computes the union)
-//   6. top-down collapse into 8-wide nodes, one tree level per launch:
-//      children are opened greedily by largest surface area while fewer than
-//      8 exist; subtrees of <= leafMax (1..3) triangles become leaves; child slots are
+//   6. SAH-optimal grouping of the binary nodes into 8-wide nodes (dynamic
+//      program of Ylitie et al. 2017 over the LBVH, bottom-up like the refit)
+//   7. top-down collapse into 8-wide nodes, one tree level per launch:
+//      children are the roots chosen by the dynamic program (or, for trees
+//      the program makes deeper than the traversal stack, opened greedily by
+//      largest surface area while fewer than 8 exist); child slots are
 //      assigned so that slot s holds the child nearest the origin of rays in
 //      direction octant s; child boxes are quantized to 8 bits per axis.
 #include <algorithm>
@@ -223,6 +226,108 @@ __global__ void k_refit(int n, const uint32_t* __restrict__ vals, const float* _
     }
 }
 
+// --- 5b. SAH-optimal grouping into 8-wide nodes ------------------------------
+//
+// Dynamic program of Ylitie, Karras and Laine (HPG 2017, sec. 4.1) over the
+// LBVH: C(u, i), i = 1..8, is the least SAH cost of representing subtree u by
+// at most i roots (children of the enclosing 8-wide node).  A leaf root costs
+// area x cTri x triangles, an 8-wide node area x cNode plus the best split of
+// its 8 slots between the binary children; C(u, i) = min(C(u, i - 1), best
+// split of i slots).  One thread per triangle walks up the tree as in k_refit;
+// the second arrival at a node evaluates it.  dec[8u + i - 1] records the
+// choice: for i = 1 whether u is best a leaf (1) or an 8-wide node (0); for
+// i >= 2 the slots j given to the left child (low 7 bits), with 0x80 set when
+// at most i - 1 roots are no worse.  Costs are relative to cNode = 1.
+#ifndef PRT_WIDE_DP
+#define PRT_WIDE_DP 1
+#endif
+#ifndef PRT_SAH_CTRI
+#define PRT_SAH_CTRI 0.7f
+#endif
+
+__device__ __forceinline__ float box_half_area(const float* b)
+{
+    float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_wide_dp(int n, const int2* __restrict__ child, const int2* __restrict__ range,
+                          const int* __restrict__ parent, const float* box, int* flag, float* cost, uint8_t* dec,
+                          int leafMax)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const size_t u0 = (size_t)(n - 1) + k;
+    float b6[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) b6[c] = __ldcg(box + 6 * u0 + c);
+    const float leafCost = box_half_area(b6) * PRT_SAH_CTRI;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        __stcg(cost + 8 * u0 + i, leafCost);
+        dec[8 * u0 + i] = i == 0 ? 1 : 0x80;
+    }
+    int node = parent[u0];
+    while (node >= 0)
+    {
+        __threadfence();
+        if (atomicAdd(&flag[node], 1) == 0) return;   // the sibling finishes this node
+        const int2 ch = child[node];
+        const size_t ua = ch.x >= 0 ? (size_t)ch.x : (size_t)(n - 1) + ~ch.x;
+        const size_t ub = ch.y >= 0 ? (size_t)ch.y : (size_t)(n - 1) + ~ch.y;
+        float ca[8], cb[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+        {
+            ca[i] = __ldcg(cost + 8 * ua + i);
+            cb[i] = __ldcg(cost + 8 * ub + i);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) b6[c] = __ldcg(box + 6 * (size_t)node + c);
+        const float area = box_half_area(b6);
+        const int2 rg = range[node];
+        const int cnt = rg.y - rg.x + 1;
+        float dist[8];
+        uint8_t split[8];
+        dist[0] = FLT_MAX;
+        split[0] = 0;
+#pragma unroll
+        for (int i = 2; i <= 8; ++i)
+        {
+            float best = FLT_MAX;
+            int bj = 1;
+#pragma unroll
+            for (int j = 1; j < i; ++j)
+            {
+                const float v = ca[j - 1] + cb[i - j - 1];
+                if (v < best)
+                {
+                    best = v;
+                    bj = j;
+                }
+            }
+            dist[i - 1] = best;
+            split[i - 1] = (uint8_t)bj;
+        }
+        const float leafOpt = cnt <= leafMax ? area * PRT_SAH_CTRI * (float)cnt : FLT_MAX;
+        const float wideOpt = area + dist[7];
+        float c = fminf(leafOpt, wideOpt);
+        __stcg(cost + 8 * (size_t)node, c);
+        dec[8 * (size_t)node] = leafOpt <= wideOpt ? 1 : 0;
+#pragma unroll
+        for (int i = 2; i <= 8; ++i)
+        {
+            uint8_t d = split[i - 1];
+            if (c <= dist[i - 1]) d |= 0x80;
+            else c = dist[i - 1];
+            __stcg(cost + 8 * (size_t)node + i - 1, c);
+            dec[8 * (size_t)node + i - 1] = d;
+        }
+        node = parent[node];
+    }
+}
+
 // --- 6. collapse into 8-wide nodes ------------------------------------------
 
 struct CollapseArgs
@@ -241,6 +346,7 @@ struct CollapseArgs
     int nodeCapacity;
     int* error;
     int leafMax;   // subtrees of at most this many triangles (1..3) become leaves
+    const uint8_t* dec;   // decisions of k_wide_dp, or nullptr for the greedy grouping
 };
 
 __device__ __forceinline__ int ref_count(const CollapseArgs& a, int ref)
@@ -248,6 +354,15 @@ __device__ __forceinline__ int ref_count(const CollapseArgs& a, int ref)
     if (ref < 0) return 1;
     int2 r = a.range[ref];
     return r.y - r.x + 1;
+}
+
+// A child of an 8-wide node is a leaf (its triangles) or an 8-wide node.
+__device__ __forceinline__ bool ref_is_leaf(const CollapseArgs& a, int ref)
+{
+    if (ref < 0) return true;
+    int2 r = a.range[ref];
+    if (r.y - r.x + 1 > a.leafMax) return false;
+    return a.dec ? a.dec[8 * (size_t)ref] == 1 : true;
 }
 
 __device__ __forceinline__ const float* ref_box(const CollapseArgs& a, int ref)
@@ -277,6 +392,38 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
     {
         ch[0] = bref;
         nc = 1;
+    }
+    else if (a.dec)
+    {
+        // the roots of the best split of 8 slots (k_wide_dp decisions)
+        int2 st[16];
+        int sp = 0;
+        const int2 c = a.child[bref];
+        const int j = a.dec[8 * (size_t)bref + 7] & 0x7f;
+        st[sp++] = make_int2(c.y, 8 - j);
+        st[sp++] = make_int2(c.x, j);
+        nc = 0;
+        while (sp > 0 && nc < 8)
+        {
+            const int2 e = st[--sp];
+            const int r = e.x, i = e.y;
+            if (r < 0 || i <= 1)
+            {
+                ch[nc++] = r;
+                continue;
+            }
+            const uint8_t d = a.dec[8 * (size_t)r + i - 1];
+            if (d & 0x80)
+            {
+                st[sp++] = make_int2(r, i - 1);
+            }
+            else
+            {
+                const int2 c2 = a.child[r];
+                st[sp++] = make_int2(c2.y, i - (int)d);
+                st[sp++] = make_int2(c2.x, (int)d);
+            }
+        }
     }
     else
     {
@@ -344,9 +491,8 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
     int nInternal = 0, nTris = 0;
     for (int i = 0; i < nc; ++i)
     {
-        int cnt = ref_count(a, ch[i]);
-        if (cnt > a.leafMax) nInternal++;
-        else nTris += cnt;
+        if (ref_is_leaf(a, ch[i])) nTris += ref_count(a, ch[i]);
+        else nInternal++;
     }
     int childBase = nInternal ? atomicAdd(a.nodeCounter, nInternal) : 0;
     int triBase = nTris ? atomicAdd(a.triCounter, nTris) : 0;
@@ -412,7 +558,7 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
             qhi[k][s] = (uint8_t)fmax(0.0, fmin(255.0, hi));
         }
         int cnt = ref_count(a, ch[i]);
-        if (cnt > a.leafMax)
+        if (!ref_is_leaf(a, ch[i]))
         {
             meta[s] = (uint8_t)(0x20 | (24 + s));
             imask |= 1u << s;
@@ -455,6 +601,47 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Runs the collapse one level per launch from the root; on success sets the
+// node and triangle counts and the number of 8-wide levels.
+int collapse_levels(const CollapseArgs& a, int2* workA, int2* workB, int* counters, int n, cudaStream_t stream,
+                    int& nodeCount, int& triCount, int& levels, std::string& err)
+{
+    int2 root = make_int2(n > 1 ? 0 : ~0, 0);
+    int init[4] = {1, 0, 0, 0};   // nodeCounter, triCounter, nextCount, error
+    int hostCounters[4];
+    cudaError_t e = cudaMemcpyAsync(workA, &root, sizeof(int2), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream);
+    levels = 0;
+    int workCount = 1;
+    while (e == cudaSuccess && workCount > 0)
+    {
+        e = cudaMemsetAsync(counters + 2, 0, sizeof(int), stream);
+        if (e != cudaSuccess) break;
+        k_collapse<<<div_up(workCount, 128), 128, 0, stream>>>(a, workA, workCount, workB, counters + 2);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(hostCounters, counters, sizeof(hostCounters), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) break;
+        ++levels;
+        if (hostCounters[3])
+        {
+            err = "BVH8 collapse exceeded its node capacity";
+            return PRT_EINTERNAL;
+        }
+        workCount = hostCounters[2];
+        std::swap(workA, workB);
+    }
+    if (e != cudaSuccess)
+    {
+        err = std::string("BVH8 collapse: ") + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA;
+    }
+    nodeCount = hostCounters[0];
+    triCount = hostCounters[1];
+    return PRT_OK;
+}
+
 } // namespace
 
 #define BUILD_CHECK(x)                                                                                          \
@@ -490,7 +677,8 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     int2 *child = nullptr, *range = nullptr, *workA = nullptr, *workB = nullptr;
     int *parent = nullptr, *flag = nullptr, *counters = nullptr;
     float* box = nullptr;
-    int hostCounters[4];
+    float* dpCost = nullptr;
+    uint8_t* dpDec = nullptr;
     int levels = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -534,12 +722,17 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     k_refit<<<div_up(n, 256), 256, 0, stream>>>(n, valsA, triBox, child, parent, box, flag);
     BUILD_CHECK(cudaGetLastError());
 
+    if (PRT_WIDE_DP && nInternal > 0)
     {
-        // collapse, one level per launch
-        int2 root = make_int2(n > 1 ? 0 : ~0, 0);
-        int init[4] = {1, 0, 0, 0};   // nodeCounter, triCounter, nextCount, error
-        BUILD_CHECK(cudaMemcpyAsync(workA, &root, sizeof(int2), cudaMemcpyHostToDevice, stream));
-        BUILD_CHECK(cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        BUILD_CHECK(dev_malloc(&dpCost, sizeof(float) * 8 * (size_t)(2 * n)));
+        BUILD_CHECK(dev_malloc(&dpDec, sizeof(uint8_t) * 8 * (size_t)(2 * n)));
+        BUILD_CHECK(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)nInternal, stream));
+        k_wide_dp<<<div_up(n, 256), 256, 0, stream>>>(n, child, range, parent, box, flag, dpCost, dpDec,
+                                                     std::max(1, std::min(3, leafMax)));
+        BUILD_CHECK(cudaGetLastError());
+    }
+
+    {
         CollapseArgs a;
         a.n = n;
         a.child = child;
@@ -555,26 +748,19 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         a.nodeCapacity = nodeCapacity;
         a.error = counters + 3;
         a.leafMax = std::max(1, std::min(3, leafMax));
-        int workCount = 1;
-        while (workCount > 0)
+        a.dec = dpDec;
+        int nodeCount = 0, triCount = 0;
+        status = collapse_levels(a, workA, workB, counters, n, stream, nodeCount, triCount, levels, err);
+        if (status == PRT_OK && a.dec && 2 * levels > kStackMax)
         {
-            BUILD_CHECK(cudaMemsetAsync(counters + 2, 0, sizeof(int), stream));
-            k_collapse<<<div_up(workCount, 128), 128, 0, stream>>>(a, workA, workCount, workB, counters + 2);
-            BUILD_CHECK(cudaGetLastError());
-            BUILD_CHECK(cudaMemcpyAsync(hostCounters, counters, sizeof(hostCounters), cudaMemcpyDeviceToHost, stream));
-            BUILD_CHECK(cudaStreamSynchronize(stream));
-            ++levels;
-            if (hostCounters[3])
-            {
-                err = "BVH8 collapse exceeded its node capacity";
-                status = PRT_EINTERNAL;
-                goto done;
-            }
-            workCount = hostCounters[2];
-            std::swap(workA, workB);
+            // the SAH grouping came out deeper than the traversal stack allows
+            // (possible for degenerate inputs): group greedily instead
+            a.dec = nullptr;
+            status = collapse_levels(a, workA, workB, counters, n, stream, nodeCount, triCount, levels, err);
         }
-        out.nodeCount = hostCounters[0];
-        out.triCount = hostCounters[1];
+        if (status != PRT_OK) goto done;
+        out.nodeCount = nodeCount;
+        out.triCount = triCount;
         out.leafMax = a.leafMax;
         out.levels = levels;
         if (out.triCount != n)
@@ -615,6 +801,8 @@ done:
     cudaFree(parent);
     cudaFree(flag);
     cudaFree(box);
+    cudaFree(dpCost);
+    cudaFree(dpDec);
     cudaFree(workA);
     cudaFree(workB);
     cudaFree(counters);

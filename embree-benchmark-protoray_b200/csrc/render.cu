@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneD
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
-    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // closest hit, leafTris == 1
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // leafTris == 1
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -514,9 +514,10 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneD
             if (exhausted) break;
             continue;
         }
-        if (!kAnyHit && PRT_DEFER_ISECT && sc.leafTris == 1)
+        if (PRT_DEFER_ISECT && sc.leafTris == 1)
         {
-            warp_trav_deferred(*tq, ts, sc, r, tnear, st, has, !exhausted, kRefillMin, lane);
+            warp_trav_deferred(*tq, ts, sc, r, tnear, st, has, !exhausted, kRefillMin, lane, nullptr, nullptr,
+                               nullptr, nullptr, nullptr, kAnyHit);
         }
         else
         for (;;)
@@ -976,7 +977,7 @@ int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n
     if (n <= 0) return 0;
     const int block = 128;
     size_t shmem = sizeof(uint2) * kShared * block;
-    if (!anyHit && PRT_DEFER_ISECT && sc.leafTris == 1) shmem += sizeof(TriQueue) * (block / 32);
+    if (PRT_DEFER_ISECT && sc.leafTris == 1) shmem += sizeof(TriQueue) * (block / 32);
     LaunchCfg cfg;
     auto go = [&](auto kernel) {
         // no more warps than rays: 32 rays per warp

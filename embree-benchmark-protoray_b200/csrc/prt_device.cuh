@@ -487,8 +487,11 @@ __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q,
 // memory (one column per thread), deeper entries spill to local memory.  A
 // node visit pushes at most one node group and one postponed triangle group,
 // so a tree of L 8-wide levels needs at most 2L entries.
-constexpr int kShared = 8;
-constexpr int kLocal = 56;
+#ifndef PRT_STACK_SHARED
+#define PRT_STACK_SHARED 8
+#endif
+constexpr int kShared = PRT_STACK_SHARED;
+constexpr int kLocal = 64 - PRT_STACK_SHARED;
 constexpr int kStackMax = kShared + kLocal;
 
 struct TravStack

@@ -657,7 +657,7 @@ int collapse_levels(const CollapseArgs& a, int2* workA, int2* workB, int* counte
     } while (0)
 
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
-               std::string& err, BuildInfo* info, int leafMax)
+               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping)
 {
     (void)nv;
     int status = PRT_OK;
@@ -722,7 +722,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     k_refit<<<div_up(n, 256), 256, 0, stream>>>(n, valsA, triBox, child, parent, box, flag);
     BUILD_CHECK(cudaGetLastError());
 
-    if (PRT_WIDE_DP && nInternal > 0)
+    if (PRT_WIDE_DP && sahGrouping && nInternal > 0)
     {
         BUILD_CHECK(dev_malloc(&dpCost, sizeof(float) * 8 * (size_t)(2 * n)));
         BUILD_CHECK(dev_malloc(&dpDec, sizeof(uint8_t) * 8 * (size_t)(2 * n)));

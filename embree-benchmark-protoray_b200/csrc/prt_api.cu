@@ -62,6 +62,7 @@ struct prt_ctx
     Bvh8Device bvh;
     bool built = false;
     int leafMax = kDefaultLeafMax;
+    bool highQuality = true;   // SAH grouping into 8-wide nodes
 
     // camera / frame
     prt_camera cam{};
@@ -825,6 +826,14 @@ int prt_set_leaf_size(prt_ctx* ctx, int maxTrianglesPerLeaf)
     return PRT_OK;
 }
 
+int prt_set_build_quality(prt_ctx* ctx, int high)
+{
+    if (!ctx) return PRT_EINVAL;
+    if (high != 0 && high != 1) return fail(ctx, PRT_EINVAL, "build quality must be 0 (low) or 1 (high)");
+    ctx->highQuality = high == 1;
+    return PRT_OK;
+}
+
 int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats)
 {
     if (!ctx) return PRT_EINVAL;
@@ -834,7 +843,8 @@ int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats)
     ctx->built = false;
     BuildInfo info;
     std::string err;
-    int st = build_bvh8(ctx->dPos, ctx->nv, ctx->dIdx, ctx->nt, ctx->bvh, ctx->stream, err, &info, ctx->leafMax);
+    int st = build_bvh8(ctx->dPos, ctx->nv, ctx->dIdx, ctx->nt, ctx->bvh, ctx->stream, err, &info, ctx->leafMax,
+                        ctx->highQuality);
     if (st != PRT_OK) return fail(ctx, st, err);
     ctx->built = true;
     if (stats)

@@ -68,7 +68,7 @@ struct BuildInfo
 };
 
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
-               std::string& err, BuildInfo* info, int leafMax);
+               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping = true);
 
 // Sort and scan primitives (sort_scan.cu).  radix_sort_pairs sorts (key, value)
 // pairs stably on key bits [0, bits); the sorted pairs end in keys/vals (the

@@ -52,6 +52,8 @@ void DeviceB200::initRenderer(const Props& props, Props& stats)
     maxDepth_ = props.getInt("maxDepth", 6);   // render/diffuse_integrator_single.h:35
     passesPerFrame_ = props.getInt("sppPerFrame", 1);
     if (passesPerFrame_ < 1) throw std::invalid_argument("sppPerFrame must be positive");
+    // -no-sbvh: the reference's switch off its high-quality build (accel/embree/embree_intersector.cpp:24)
+    check(prt_set_build_quality(ctx_, props.exists("no-sbvh") ? 0 : 1));
     prt_build_stats bs;
     check(prt_build_accel(ctx_, &bs));
     stats.set("buildMs", bs.buildMs);

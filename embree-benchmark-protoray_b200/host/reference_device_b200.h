@@ -61,6 +61,7 @@ public:
         accumulate = type == "diffuse" || type == "diffuse2";
         check(prt_set_integrator(ctx, type.rfind("diffuse2", 0) == 0 ? PRT_INTEGRATOR_DIFFUSE2 : PRT_INTEGRATOR_DIFFUSE));
         maxDepth = props.get("maxDepth", 6);
+        check(prt_set_build_quality(ctx, props.exists("no-sbvh") ? 0 : 1));
         prt_build_stats bs;
         check(prt_build_accel(ctx, &bs));
         stats.set("buildMs", bs.buildMs);

@@ -30,7 +30,7 @@ EXPORTS = [
     "prt_create", "prt_destroy", "prt_last_error", "prt_get_info",
     "prt_load_mesh", "prt_load_mesh_file", "prt_get_scene_bounds", "prt_set_albedo", "prt_set_sky",
     "prt_set_integrator",
-    "prt_build_accel", "prt_set_leaf_size", "prt_camera_from_view", "prt_set_camera",
+    "prt_build_accel", "prt_set_leaf_size", "prt_set_build_quality", "prt_camera_from_view", "prt_set_camera",
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
@@ -119,6 +119,7 @@ def lib() -> C.CDLL:
         "prt_set_integrator": (ip, [vp, ip]),
         "prt_build_accel": (ip, [vp, C.POINTER(BuildStats)]),
         "prt_set_leaf_size": (ip, [vp, ip]),
+        "prt_set_build_quality": (ip, [vp, ip]),
         "prt_camera_from_view": (ip, [C.POINTER(View), ip, ip, C.POINTER(Camera)]),
         "prt_set_camera": (ip, [vp, C.POINTER(Camera)]),
         "prt_init_frame": (ip, [vp, ip, ip]),
@@ -275,6 +276,10 @@ class Context:
 
     def set_leaf_size(self, n: int):
         self._check(self.L.prt_set_leaf_size(self.h, n), "prt_set_leaf_size")
+
+    def set_build_quality(self, high: bool):
+        """True: SAH grouping into 8-wide nodes (default); False: greedy."""
+        self._check(self.L.prt_set_build_quality(self.h, 1 if high else 0), "prt_set_build_quality")
 
     def build(self) -> Dict[str, float]:
         s = BuildStats()

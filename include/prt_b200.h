@@ -146,6 +146,12 @@ int prt_set_integrator(prt_ctx* ctx, int integrator);
 int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats);
 /* Largest leaf of the 8-wide tree, 1..3 triangles, for the next build. */
 int prt_set_leaf_size(prt_ctx* ctx, int maxTrianglesPerLeaf);
+/* Build quality for the next build, the reference's high-quality switch
+ * (`-no-sbvh` turns it off, accel/embree/embree_intersector.cpp:24,56-57):
+ * high (1, the default) groups the LBVH into 8-wide nodes by the SAH dynamic
+ * program; low (0) opens the largest child greedily, which is faster to build
+ * and gives a tree of more, emptier nodes. */
+int prt_set_build_quality(prt_ctx* ctx, int high);
 
 /* --- camera (DeviceCuda::initCamera, render/device_cuda.cpp:175-200) --- */
 /* Builds the camera of a view for an image of width x height, as the

@@ -25,9 +25,10 @@ def _decode(nodes):
     return origin, scale, imask, child, tbase, meta, qlo, qhi
 
 
-@pytest.mark.parametrize("scene,leaf", [("small", 1), ("small", 3), ("batch3", 1), ("batch3", 2), ("one", 1),
-                                        ("two", 1), ("two", 3)])
-def test_bvh_structure(scene, leaf, small):
+@pytest.mark.parametrize("scene,leaf,high", [("small", 1, 1), ("small", 3, 1), ("batch3", 1, 1), ("batch3", 2, 1),
+                                             ("one", 1, 1), ("two", 1, 1), ("two", 3, 1), ("small", 1, 0),
+                                             ("batch3", 2, 0)])
+def test_bvh_structure(scene, leaf, high, small):
     import prt
     import scenes
     if scene == "small":
@@ -45,6 +46,7 @@ def test_bvh_structure(scene, leaf, small):
     c = prt.Context(0)
     c.load_mesh(idx, pos)
     c.set_leaf_size(leaf)
+    c.set_build_quality(bool(high))
     st = c.build()
     nodes, tris = c.read_accel()
     assert 2 * st["levels"] <= 64
@@ -94,3 +96,32 @@ def test_bvh_structure(scene, leaf, small):
         assert rank == bin(int(imask[i])).count("1")
     assert np.all(seen_nodes == 1)
     assert np.all(seen_tris == 1)
+
+
+def test_build_quality_changes_grouping_not_hits(small):
+    """The SAH grouping (high quality, default) makes fewer, fuller 8-wide
+    nodes than the greedy one (low quality, `-no-sbvh`); closest hits and the
+    image are the same for both."""
+    import prt
+    mesh, view = small
+    W, H = 96, 96
+    out = {}
+    for high in (True, False):
+        c = prt.Context(0)
+        c.load_mesh(mesh.indices, mesh.positions)
+        c.set_build_quality(high)
+        st = c.build()
+        c.init_frame(W, H)
+        c.set_view(view, W, H)
+        r = c.render(4, 5)
+        out[high] = (st["nodeCount"], c.read_accum(), r["ray"])
+        c.close()
+    assert out[True][0] < 0.8 * out[False][0]
+    a, b = out[True][1][..., 0], out[False][1][..., 0]
+    assert float(np.mean(np.abs(a - b) / np.maximum(a, 1e-2))) < 1e-4
+    assert abs(out[True][2] - out[False][2]) <= 1e-4 * out[True][2]
+    c = prt.Context(0)
+    with pytest.raises(prt.PrtError):
+        c._check(c.L.prt_set_build_quality(c.h, 2), "prt_set_build_quality")
+    c.close()
+

@@ -702,8 +702,15 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     BUILD_CHECK(dev_malloc(&workA, sizeof(int2) * (size_t)nodeCapacity));
     BUILD_CHECK(dev_malloc(&workB, sizeof(int2) * (size_t)nodeCapacity));
     BUILD_CHECK(dev_malloc(&counters, sizeof(int) * 4));
-    BUILD_CHECK(dev_malloc(&out.nodes, sizeof(Bvh8Node) * (size_t)nodeCapacity));
-    BUILD_CHECK(dev_malloc(&out.tris, sizeof(TriRec) * (size_t)n));
+    {
+        const size_t nodeBytes = (sizeof(Bvh8Node) * (size_t)nodeCapacity + 255) & ~(size_t)255;
+        out.bytes = nodeBytes + sizeof(TriRec) * (size_t)n;
+        char* blk = nullptr;
+        BUILD_CHECK(dev_malloc(&blk, out.bytes));
+        out.block = blk;
+        out.nodes = reinterpret_cast<Bvh8Node*>(blk);
+        out.tris = reinterpret_cast<TriRec*>(blk + nodeBytes);
+    }
 
     k_tri_boxes<<<boundBlocks, 256, 0, stream>>>(dPos, dIdx, n, triBox, partial);
     k_reduce_bounds<<<1, 256, 0, stream>>>(partial, boundBlocks, cbounds);

@@ -41,10 +41,14 @@ inline cudaError_t host_pinned_alloc(char** p, size_t bytes)
     return cudaHostAlloc(reinterpret_cast<void**>(p), bytes, cudaHostAllocDefault);
 }
 
+// The 8-wide nodes and the leaf triangles live in one allocation (nodes
+// first, 256-byte aligned).
 struct Bvh8Device
 {
     Bvh8Node* nodes = nullptr;
     TriRec* tris = nullptr;
+    void* block = nullptr;   // the allocation holding both
+    size_t bytes = 0;        // its size
     int nodeCount = 0;
     int triCount = 0;
     int levels = 0;
@@ -52,10 +56,11 @@ struct Bvh8Device
 
     void release()
     {
-        if (nodes) cudaFree(nodes);
-        if (tris) cudaFree(tris);
+        if (block) cudaFree(block);
+        block = nullptr;
         nodes = nullptr;
         tris = nullptr;
+        bytes = 0;
         nodeCount = triCount = levels = 0;
     }
 };

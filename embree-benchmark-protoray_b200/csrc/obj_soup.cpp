@@ -19,6 +19,7 @@
 // are not split at 256 KiB.
 #include <algorithm>
 #include <cerrno>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -27,11 +28,36 @@
 #include <thread>
 #include <vector>
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <unistd.h>
+
 #include "../../include/prt_b200.h"
+
+namespace {
+
+// Large host buffers (the file text, the soup) on 2 MiB-aligned memory with
+// transparent huge pages requested: a 138 MB soup is then 69 page faults, not
+// 34,000, and the threads that write it do not queue on the page-table lock.
+struct HugeFree
+{
+    void operator()(void* p) const { std::free(p); }
+};
+
+void* huge_alloc(size_t bytes)
+{
+    const size_t align = size_t(2) << 20;
+    const size_t n = (std::max<size_t>(bytes, 1) + align - 1) / align * align;
+    void* p = std::aligned_alloc(align, n);
+    if (p) madvise(p, n, MADV_HUGEPAGE);
+    return p;
+}
+
+} // namespace
 
 struct prt_soup
 {
-    std::unique_ptr<prt_soup_triangle[]> tris;
+    std::unique_ptr<prt_soup_triangle, HugeFree> tris;
     long long triCount = 0;
     std::vector<std::string> names;
     long long degenerate = 0;
@@ -43,11 +69,98 @@ inline bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\
 // strtok delimiters of the face parser (obj_loader.cpp:163)
 inline bool is_face_delim(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r'; }
 
-// sscanf "%f": skips white space, then strtof.  `end` bounds the line.
+// Decimal -> float with the result of strtof, for the common case.  A
+// decimal number w x 10^q with w < 2^53 and |q| <= 22 converts to the nearest
+// double with one IEEE multiply or divide of exact operands (Clinger,
+// "How to read floating point numbers accurately", PLDI 1990).  Rounding that
+// double to float gives the nearest float unless the double lies exactly on a
+// midpoint between two floats (every float midpoint is a double, so no other
+// midpoint can separate the double from the exact value); that case, numbers
+// outside the normal float range, more than 19 significant digits, hex,
+// inf and nan return false and are left to strtof.  On success `next` is the
+// first character after the number, as strtof's end pointer.
+bool fast_decimal_float(const char* s, const char* end, float& out, const char*& next)
+{
+    static const double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                                      1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+    const char* p = s;
+    bool neg = false;
+    if (p < end && (*p == '+' || *p == '-')) neg = *p++ == '-';
+    if (p + 1 < end && p[0] == '0' && (p[1] == 'x' || p[1] == 'X')) return false;
+    uint64_t w = 0;
+    int digits = 0, q = 0;
+    bool any = false;
+    while (p < end && *p >= '0' && *p <= '9')
+    {
+        any = true;
+        if (w != 0 || *p != '0')
+        {
+            if (++digits > 19) return false;
+            w = w * 10 + (uint64_t)(*p - '0');
+        }
+        ++p;
+    }
+    if (p < end && *p == '.')
+    {
+        ++p;
+        while (p < end && *p >= '0' && *p <= '9')
+        {
+            any = true;
+            if (w != 0 || *p != '0')
+            {
+                if (++digits > 19) return false;
+                w = w * 10 + (uint64_t)(*p - '0');
+            }
+            --q;
+            ++p;
+        }
+    }
+    if (!any) return false;
+    if (p < end && (*p == 'e' || *p == 'E'))
+    {
+        const char* e = p + 1;
+        bool eneg = false;
+        if (e < end && (*e == '+' || *e == '-')) eneg = *e++ == '-';
+        if (e < end && *e >= '0' && *e <= '9')
+        {
+            int x = 0;
+            while (e < end && *e >= '0' && *e <= '9')
+            {
+                if (x < 100000) x = x * 10 + (*e - '0');
+                ++e;
+            }
+            q += eneg ? -x : x;
+            p = e;
+        }
+    }
+    next = p;
+    if (w == 0)
+    {
+        out = neg ? -0.0f : 0.0f;
+        return true;
+    }
+    if (w > (1ULL << 53) || q < -22 || q > 22) return false;
+    double d = (double)w;
+    d = q >= 0 ? d * kPow10[q] : d / kPow10[-q];
+    if (d > 3.4028234663852886e38 || d < 1.1754943508222875e-38) return false;   // overflow or subnormal
+    uint64_t bits;
+    std::memcpy(&bits, &d, 8);
+    if ((bits & ((1ULL << 29) - 1)) == (1ULL << 28)) return false;   // exactly halfway between two floats
+    out = neg ? -(float)d : (float)d;
+    return true;
+}
+
+// sscanf "%f": skips white space, then converts as strtof.  `end` bounds the line.
 bool scan_float(const char*& s, const char* end, float& out)
 {
     while (s < end && is_ws(*s)) ++s;
     if (s >= end) return false;
+    const char* next = nullptr;
+    if (fast_decimal_float(s, end, out, next))
+    {
+        s = next;
+        return true;
+    }
     char* e = nullptr;
     out = std::strtof(s, &e);
     if (e == s || e > end) return false;
@@ -77,8 +190,16 @@ bool scan_corner(const char* s, const char* end, int& p, int& t, int& n)
 {
     const char* q = s;
     int a, b, c;
+    if (!scan_int(q, end, a)) return false;
+    if (q >= end || *q != '/')
+    {
+        // a plain position index: every pattern stops after the first number
+        p = a;
+        t = 0;
+        n = 0;
+        return true;
+    }
     // "%d/%d/%d"
-    if (scan_int(q, end, a) && q < end && *q == '/')
     {
         const char* r = q + 1;
         if (scan_int(r, end, b) && r < end && *r == '/')
@@ -155,6 +276,11 @@ struct Chunk
 
 void parse_chunk(Chunk& c)
 {
+    // capacity guesses from the chunk size (a face or vertex line is >= 8 bytes)
+    const size_t lines = (size_t)(c.end - c.begin) / 16 + 16;
+    c.v.reserve(3 * lines);
+    c.corners.reserve(3 * lines);
+    c.faces.reserve(lines);
     const char* s = c.begin;
     while (s < c.end)
     {
@@ -176,7 +302,9 @@ void parse_chunk(Chunk& c)
                 c.error = "Invalid vertex position";
                 return;
             }
-            c.v.insert(c.v.end(), {x, y, z});
+            c.v.push_back(x);
+            c.v.push_back(y);
+            c.v.push_back(z);
         }
         else if (hl == 2 && h[0] == 'v' && h[1] == 'n')
         {
@@ -186,7 +314,9 @@ void parse_chunk(Chunk& c)
                 c.error = "Invalid vertex normal";
                 return;
             }
-            c.vn.insert(c.vn.end(), {x, y, z});
+            c.vn.push_back(x);
+            c.vn.push_back(y);
+            c.vn.push_back(z);
         }
         else if (hl == 2 && h[0] == 'v' && h[1] == 't')
         {
@@ -196,7 +326,8 @@ void parse_chunk(Chunk& c)
                 c.error = "Invalid vertex texture coordinates";
                 return;
             }
-            c.vt.insert(c.vt.end(), {x, y});
+            c.vt.push_back(x);
+            c.vt.push_back(y);
         }
         else if (hl == 1 && h[0] == 'f')
         {
@@ -217,7 +348,9 @@ void parse_chunk(Chunk& c)
                 while (te < eol && !is_face_delim(*te)) ++te;
                 int p = 0, tx = 0, n = 0;
                 if (!scan_corner(t, te, p, tx, n)) ok = false;
-                c.corners.insert(c.corners.end(), {p, tx, n});
+                c.corners.push_back(p);
+                c.corners.push_back(tx);
+                c.corners.push_back(n);
                 ++f.count;
                 t = te;
             }
@@ -332,26 +465,44 @@ int prt_soup_load_obj(const char* path, int threads, prt_soup** soupOut, char* e
 {
     if (!path || !soupOut) return PRT_EINVAL;
     *soupOut = nullptr;
-    FILE* f = std::fopen(path, "rb");
-    if (!f)
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0)
     {
         set_err(err, errlen, std::string("Could not open OBJ file: ") + path);
         return PRT_EIO;
     }
-    std::fseek(f, 0, SEEK_END);
-    const long long size = std::ftell(f);
-    std::fseek(f, 0, SEEK_SET);
-    std::unique_ptr<char[]> text(new char[(size_t)size + 1]);
-    const bool readOk = size >= 0 && std::fread(text.get(), 1, (size_t)size, f) == (size_t)size;
-    std::fclose(f);
+    const long long size = (long long)::lseek(fd, 0, SEEK_END);
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::unique_ptr<char, HugeFree> text(static_cast<char*>(huge_alloc((size_t)std::max(0LL, size) + 1)));
+    bool readOk = size >= 0 && text;
+    if (readOk)
+    {
+        // the file in parallel pieces of at least 4 MiB
+        const int pieces = (int)std::max(1LL, std::min<long long>(threads, size >> 22));
+        std::vector<char> ok((size_t)pieces, 1);
+        parallel(pieces, pieces, [&](int i) {
+            long long at = size * i / pieces, stop = size * (i + 1) / pieces;
+            while (at < stop)
+            {
+                ssize_t got = ::pread(fd, text.get() + at, (size_t)(stop - at), (off_t)at);
+                if (got <= 0)
+                {
+                    ok[(size_t)i] = 0;
+                    return;
+                }
+                at += got;
+            }
+        });
+        for (char k : ok) readOk = readOk && k;
+    }
+    ::close(fd);
     if (!readOk)
     {
         set_err(err, errlen, std::string("read error: ") + path);
         return PRT_EIO;
     }
-    text[(size_t)size] = '\0';
+    text.get()[(size_t)size] = '\0';
 
-    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     const long long minChunk = 64 << 10;
     const int nChunks = (int)std::max(1LL, std::min<long long>(4LL * threads, size / minChunk));
     std::vector<Chunk> chunks((size_t)nChunks);
@@ -448,7 +599,12 @@ int prt_soup_load_obj(const char* path, int threads, prt_soup** soupOut, char* e
         set_err(err, errlen, "too many triangles");
         return PRT_EIO;
     }
-    soup->tris.reset(new prt_soup_triangle[(size_t)std::max(1LL, total)]);
+    soup->tris.reset(static_cast<prt_soup_triangle*>(huge_alloc(sizeof(prt_soup_triangle) * (size_t)total)));
+    if (!soup->tris)
+    {
+        set_err(err, errlen, "out of host memory");
+        return PRT_EIO;
+    }
     soup->triCount = total;
     soup->degenerate = degenerate;
     parallel(nChunks, threads, [&](int i) {

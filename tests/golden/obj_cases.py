@@ -89,6 +89,14 @@ def obj_cases() -> List[Tuple[str, str]]:
     c.append(("forward_reference", "f 1 2 3\nf 3 2 4\nv 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 1\n"))
     c.append(("empty", ""))
     c.append(("comments_only", "# nothing\n\n# more\n"))
+    c.append(("numbers",                                  # decimal -> float edge cases
+              "v 16777217 0.1 -0.0\nv 1e22 1e23 3.4028235e38\nv 1e-45 1.4e-45 1e-38\n"
+              "v 123456789012345678901234 0.000000000000000000000001 9007199254740993\n"
+              "v .5 5. +1.5e+3\nv 1E3 2e-0 0e9\nv 0x1p3 0X1.8P-2 -0x10\n"
+              "v 0.12345678901234567890123 -7.0000005 33554431\n"
+              "v 1.00000005960464477539062 3.4028235e38 -1.17549435e-38\n"
+              "f 1 2 3\nf 4 5 6\nf 7 8 9\n"))
+    c.append(("nonfinite", "v 0 0 0\nv inf 1 nan\nv 1 3.4028236e38 -INFINITY\nf 1 2 3\n"))
     c.append(("grid", _grid_obj(24, 20, seed=7)))
     c.append(("grid_plain", _grid_obj(40, 30, seed=8, forms=False, materials=0)))
     # files the reference rejects

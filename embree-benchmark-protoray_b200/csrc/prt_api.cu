@@ -13,6 +13,7 @@
 #include <fstream>
 #include <functional>
 #include <memory>
+#include <new>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -1518,19 +1519,17 @@ int prt_save_built_mesh(prt_ctx* ctx, const char* path)
     const BuiltMesh& m = ctx->builtMesh;
     if (!m.valid) return fail(ctx, PRT_ESTATE, "no mesh has been built");
     CK(cudaSetDevice(ctx->device));
-    // the blob in one pinned buffer: header, indices, material ids, attributes, names
+    // the blob in one host buffer: header, indices, material ids, attributes,
+    // names (ordinary memory: pinning a buffer for one copy costs more than
+    // the pageable copy saves)
     const size_t idxBytes = 12 * (size_t)m.triCount, matBytes = 4 * (size_t)m.triCount;
     const size_t attrBytes = sizeof(float) * m.stride * (size_t)m.vertCount;
     size_t namesBytes = 4;
     for (const std::string& s : m.names) namesBytes += 4 + s.size();
     const size_t total = 38 + idxBytes + matBytes + attrBytes + namesBytes;
-    char* buf = nullptr;
-    CK(host_pinned_alloc(&buf, total));
-    struct Freer
-    {
-        char* p;
-        ~Freer() { cudaFreeHost(p); }
-    } freer{buf};
+    std::unique_ptr<char[]> owner(new (std::nothrow) char[total]);
+    char* buf = owner.get();
+    if (!buf) return fail(ctx, PRT_ENOMEM, "cannot allocate the host blob buffer");
     const int id = 0x04df8666, tri = m.triCount, vert = m.vertCount;
     std::memcpy(buf, &id, 4);
     std::memcpy(buf + 4, m.lo, 12);

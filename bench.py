@@ -345,8 +345,9 @@ def run_fwd_bwd(prt, torch, device):
 
 def run_mesh_build(prt, torch, device):
     """`protoray build` of the terrain scene written as an OBJ (positions and
-    faces, 52 MB): OBJ parse on host threads, GPU mesh build (de-duplication +
-    Morton reorder), .mesh write; beside it the reference's ObjLoader and
+    faces, 52 MB): OBJ parse on host threads, GPU mesh build from the OBJ's
+    indexed form (upload, expansion, de-duplication, Morton reorder), .mesh
+    write; beside it the reference's ObjLoader and
     TriangleMeshBuilder (one host thread each) on the same file, when the
     reference build is present."""
     import shutil
@@ -363,10 +364,11 @@ def run_mesh_build(prt, torch, device):
         best = None
         for _ in range(4):
             t0 = time.perf_counter()
-            tris, names, _ = prt.load_obj(obj)
+            soup = prt.Soup(obj)
             t1 = time.perf_counter()
-            info = c.build_mesh(tris, names)
+            info = c.build_mesh_soup(soup)
             t2 = time.perf_counter()
+            soup.close()
             c.save_built_mesh(os.path.join(d, "terrain.mesh"))
             t3 = time.perf_counter()
             r = {"parse_ms": (t1 - t0) * 1e3, "build_device_ms": info["buildMs"], "build_ms": (t2 - t1) * 1e3,

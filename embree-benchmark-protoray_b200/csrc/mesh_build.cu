@@ -339,10 +339,38 @@ __global__ void __launch_bounds__(256) k_tri_emit(const uint32_t* __restrict__ o
     mat[j] = (*flags & kFlagMaterials) ? __float_as_int(soup[kSoupFloats * t + 24]) : 0;
 }
 
+// 0. expansion of an indexed soup into 100-byte triangle records on the device
+
+__global__ void __launch_bounds__(256) k_soup_expand(const float* __restrict__ v, const float* __restrict__ vt,
+                                                   const float* __restrict__ vn, const int* __restrict__ corners,
+                                                   int cornerInts, const int* __restrict__ mat, int n,
+                                                   float* __restrict__ soup)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int* c = corners + 3 * cornerInts * t;
+    float* o = soup + kSoupFloats * t;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        const long long p = c[cornerInts * k];
+        const int tx = cornerInts == 3 ? c[3 * k + 1] : -1, nr = cornerInts == 3 ? c[3 * k + 2] : -1;
+        o[8 * k + 0] = v[3 * p];
+        o[8 * k + 1] = v[3 * p + 1];
+        o[8 * k + 2] = v[3 * p + 2];
+        o[8 * k + 3] = nr >= 0 ? vn[3 * (long long)nr] : 0.f;
+        o[8 * k + 4] = nr >= 0 ? vn[3 * (long long)nr + 1] : 0.f;
+        o[8 * k + 5] = nr >= 0 ? vn[3 * (long long)nr + 2] : 0.f;
+        o[8 * k + 6] = tx >= 0 ? vt[2 * (long long)tx] : 0.f;
+        o[8 * k + 7] = tx >= 0 ? vt[2 * (long long)tx + 1] : 0.f;
+    }
+    o[24] = __int_as_float(mat[t]);
+}
+
 } // namespace
 
 int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream, BuiltMesh& out, std::string& err,
-                   double* buildMs, long long* launchesOut)
+                   double* buildMs, long long* launchesOut, bool soupOnDevice)
 {
     out.release();
     if (n < 0 || n > 0x7fffffff / 3)
@@ -391,7 +419,8 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
     if (n > 0)
     {
         const size_t hc = radix_sort_hist_entries(std::max(n, nc));
-        MB_CHECK(dev_malloc(&soup, sizeof(prt_soup_triangle) * (size_t)n));
+        if (soupOnDevice) soup = const_cast<float*>(reinterpret_cast<const float*>(hostTris));
+        else MB_CHECK(dev_malloc(&soup, sizeof(prt_soup_triangle) * (size_t)n));
         MB_CHECK(dev_malloc(&corners, sizeof(float4) * 2 * (size_t)nc));
         MB_CHECK(dev_malloc(&triKeys, sizeof(uint32_t) * (size_t)n));
         MB_CHECK(dev_malloc(&triVals, sizeof(uint32_t) * (size_t)n));
@@ -404,7 +433,8 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
         MB_CHECK(dev_malloc(&unique, sizeof(uint32_t) * (size_t)nc));
         MB_CHECK(dev_malloc(&pos, sizeof(uint32_t) * (size_t)nc));
         MB_CHECK(dev_malloc(&sums, sizeof(uint32_t) * scan_sums_entries(nc)));
-        MB_CHECK(cudaMemcpyAsync(soup, hostTris, sizeof(prt_soup_triangle) * (size_t)n, cudaMemcpyDefault, stream));
+        if (!soupOnDevice)
+            MB_CHECK(cudaMemcpyAsync(soup, hostTris, sizeof(prt_soup_triangle) * (size_t)n, cudaMemcpyDefault, stream));
     }
     MB_CHECK(cudaMemsetAsync(small, 0, sizeof(unsigned) * 2, stream));
     MB_CHECK(cudaEventRecord(ev0, stream));
@@ -480,7 +510,7 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
 
 done:
 #undef MB_CHECK
-    cudaFree(soup);
+    if (!soupOnDevice) cudaFree(soup);
     cudaFree(partial);
     cudaFree(bounds);
     cudaFree(small);
@@ -500,6 +530,59 @@ done:
     if (ev1) cudaEventDestroy(ev1);
     if (status != PRT_OK) out.release();
     if (launchesOut) *launchesOut += launches;
+    return status;
+}
+
+int build_mesh_gpu_indexed(const SoupIndexed& s, cudaStream_t stream, BuiltMesh& out, std::string& err, double* buildMs,
+                           long long* launchesOut)
+{
+    out.release();
+    if (s.triCount < 0 || s.triCount > 0x7fffffff / 3)
+    {
+        err = "triangle count out of range";
+        return PRT_EINVAL;
+    }
+    const int n = (int)s.triCount;
+    if (n == 0) return build_mesh_gpu(nullptr, 0, stream, out, err, buildMs, launchesOut, false);
+    int status = PRT_OK;
+    float *dv = nullptr, *dvt = nullptr, *dvn = nullptr, *dsoup = nullptr;
+    int *dcorners = nullptr, *dmat = nullptr;
+    const size_t cornerBytes = sizeof(int) * 3 * (size_t)s.cornerInts * (size_t)n;
+    cudaError_t e = dev_malloc(&dv, sizeof(float) * 3 * (size_t)std::max(1LL, s.nv));
+    if (e == cudaSuccess && s.nvt) e = dev_malloc(&dvt, sizeof(float) * 2 * (size_t)s.nvt);
+    if (e == cudaSuccess && s.nvn) e = dev_malloc(&dvn, sizeof(float) * 3 * (size_t)s.nvn);
+    if (e == cudaSuccess) e = dev_malloc(&dcorners, cornerBytes);
+    if (e == cudaSuccess) e = dev_malloc(&dmat, sizeof(int) * (size_t)n);
+    if (e == cudaSuccess) e = dev_malloc(&dsoup, sizeof(prt_soup_triangle) * (size_t)n);
+    if (e == cudaSuccess && s.nv) e = cudaMemcpyAsync(dv, s.v, sizeof(float) * 3 * (size_t)s.nv, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && s.nvt)
+        e = cudaMemcpyAsync(dvt, s.vt, sizeof(float) * 2 * (size_t)s.nvt, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && s.nvn)
+        e = cudaMemcpyAsync(dvn, s.vn, sizeof(float) * 3 * (size_t)s.nvn, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dcorners, s.corners, cornerBytes, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dmat, s.mat, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+    {
+        k_soup_expand<<<div_up(n, 256), 256, 0, stream>>>(dv, dvt, dvn, dcorners, s.cornerInts, dmat, n, dsoup);
+        if (launchesOut) ++*launchesOut;
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess)
+    {
+        err = std::string("indexed soup upload: ") + cudaGetErrorString(e);
+        status = e == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA;
+    }
+    else
+    {
+        status = build_mesh_gpu(reinterpret_cast<const prt_soup_triangle*>(dsoup), n, stream, out, err, buildMs,
+                                launchesOut, true);
+    }
+    cudaFree(dv);
+    cudaFree(dvt);
+    cudaFree(dvn);
+    cudaFree(dcorners);
+    cudaFree(dmat);
+    cudaFree(dsoup);
     return status;
 }
 

@@ -33,6 +33,7 @@
 #include <unistd.h>
 
 #include "../../include/prt_b200.h"
+#include "soup_view.h"
 
 namespace {
 
@@ -55,12 +56,19 @@ void* huge_alloc(size_t bytes)
 
 } // namespace
 
+// A parsed OBJ: its vertex lists, each triangle's resolved corner indices and
+// material id (the indexed form the GPU builder uploads), and the expanded
+// 100-byte triangle records, made on the first prt_soup_triangles call.
 struct prt_soup
 {
-    std::unique_ptr<prt_soup_triangle, HugeFree> tris;
+    std::vector<float> v, vt, vn;
+    std::unique_ptr<int, HugeFree> corners;   // 3 x cornerInts per triangle
+    std::unique_ptr<int, HugeFree> mat;
+    int cornerInts = 1;
     long long triCount = 0;
     std::vector<std::string> names;
     long long degenerate = 0;
+    std::unique_ptr<prt_soup_triangle, HugeFree> tris;   // expanded on demand
 };
 
 namespace {
@@ -382,8 +390,10 @@ void parse_chunk(Chunk& c)
 inline long long convert_index(int i, long long size) { return i >= 0 ? (long long)i : (long long)i + size + 1; }
 
 // Pass 3: one sweep counts (out == nullptr), the second writes.
-void emit_chunk(Chunk& c, long long nv, long long nvt, long long nvn, const float* v, const float* vt, const float* vn,
-                prt_soup_triangle* out)
+// Pass 3: one sweep counts (corners == nullptr), the second writes each kept
+// triangle's 0-based corner indices (position only, or position, texcoord and
+// normal with -1 for none) and material id.
+void emit_chunk(Chunk& c, long long nv, long long nvt, long long nvn, int cornerInts, int* corners, int* mats)
 {
     long long tri = 0, degenerate = 0;
     for (const Face& f : c.faces)
@@ -415,18 +425,19 @@ void emit_chunk(Chunk& c, long long nv, long long nvt, long long nvn, const floa
                     return;
                 }
             }
-            if (out)
+            if (corners)
             {
-                prt_soup_triangle& o = out[c.triBase + tri];
+                int* o = corners + (size_t)3 * cornerInts * (size_t)(c.triBase + tri);
                 for (int k = 0; k < 3; ++k)
                 {
-                    std::memcpy(o.v[k].pos, v + 3 * (P[k] - 1), 12);
-                    if (N[k]) std::memcpy(o.v[k].normal, vn + 3 * (N[k] - 1), 12);
-                    else std::memset(o.v[k].normal, 0, 12);
-                    if (T[k]) std::memcpy(o.v[k].tex, vt + 2 * (T[k] - 1), 8);
-                    else std::memset(o.v[k].tex, 0, 8);
+                    o[cornerInts * k] = (int)(P[k] - 1);
+                    if (cornerInts == 3)
+                    {
+                        o[3 * k + 1] = (int)(T[k] - 1);
+                        o[3 * k + 2] = (int)(N[k] - 1);
+                    }
                 }
-                o.matId = mat;
+                mats[c.triBase + tri] = mat;
             }
             ++tri;
         }
@@ -580,8 +591,7 @@ int prt_soup_load_obj(const char* path, int threads, prt_soup** soupOut, char* e
     });
 
     // pass 3: count, then write at each chunk's offset
-    parallel(nChunks, threads,
-             [&](int i) { emit_chunk(chunks[(size_t)i], nv, nvt, nvn, v.data(), vt.data(), vn.data(), nullptr); });
+    parallel(nChunks, threads, [&](int i) { emit_chunk(chunks[(size_t)i], nv, nvt, nvn, 1, nullptr, nullptr); });
     long long total = 0, degenerate = 0;
     for (Chunk& c : chunks)
     {
@@ -599,17 +609,23 @@ int prt_soup_load_obj(const char* path, int threads, prt_soup** soupOut, char* e
         set_err(err, errlen, "too many triangles");
         return PRT_EIO;
     }
-    soup->tris.reset(static_cast<prt_soup_triangle*>(huge_alloc(sizeof(prt_soup_triangle) * (size_t)total)));
-    if (!soup->tris)
+    const int cornerInts = (nvt == 0 && nvn == 0) ? 1 : 3;
+    soup->corners.reset(static_cast<int*>(huge_alloc(sizeof(int) * 3 * cornerInts * (size_t)total)));
+    soup->mat.reset(static_cast<int*>(huge_alloc(sizeof(int) * (size_t)total)));
+    if (!soup->corners || !soup->mat)
     {
         set_err(err, errlen, "out of host memory");
         return PRT_EIO;
     }
+    soup->cornerInts = cornerInts;
     soup->triCount = total;
     soup->degenerate = degenerate;
     parallel(nChunks, threads, [&](int i) {
-        emit_chunk(chunks[(size_t)i], nv, nvt, nvn, v.data(), vt.data(), vn.data(), soup->tris.get());
+        emit_chunk(chunks[(size_t)i], nv, nvt, nvn, cornerInts, soup->corners.get(), soup->mat.get());
     });
+    soup->v = std::move(v);
+    soup->vt = std::move(vt);
+    soup->vn = std::move(vn);
     *soupOut = soup.release();
     return PRT_OK;
 }
@@ -623,7 +639,41 @@ int prt_soup_info(const prt_soup* soup, int* triCount, int* materialCount, int* 
     return PRT_OK;
 }
 
-const prt_soup_triangle* prt_soup_triangles(const prt_soup* soup) { return soup ? soup->tris.get() : nullptr; }
+const prt_soup_triangle* prt_soup_triangles(const prt_soup* soup)
+{
+    if (!soup) return nullptr;
+    prt_soup* s = const_cast<prt_soup*>(soup);   // the expansion is a cache of the indexed form
+    if (!s->tris && s->triCount > 0)
+    {
+        std::unique_ptr<prt_soup_triangle, HugeFree> t(
+            static_cast<prt_soup_triangle*>(huge_alloc(sizeof(prt_soup_triangle) * (size_t)s->triCount)));
+        if (!t) return nullptr;
+        const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
+        const long long n = s->triCount;
+        const int parts = (int)std::max(1LL, std::min<long long>(4LL * threads, n / 4096));
+        parallel(parts, threads, [&](int i) {
+            const long long b = n * i / parts, e = n * (i + 1) / parts;
+            const int ci = s->cornerInts;
+            for (long long k = b; k < e; ++k)
+            {
+                prt_soup_triangle& o = t.get()[k];
+                const int* c = s->corners.get() + (size_t)3 * ci * (size_t)k;
+                for (int j = 0; j < 3; ++j)
+                {
+                    std::memcpy(o.v[j].pos, s->v.data() + 3 * (size_t)c[ci * j], 12);
+                    const int tx = ci == 3 ? c[3 * j + 1] : -1, nr = ci == 3 ? c[3 * j + 2] : -1;
+                    if (nr >= 0) std::memcpy(o.v[j].normal, s->vn.data() + 3 * (size_t)nr, 12);
+                    else std::memset(o.v[j].normal, 0, 12);
+                    if (tx >= 0) std::memcpy(o.v[j].tex, s->vt.data() + 2 * (size_t)tx, 8);
+                    else std::memset(o.v[j].tex, 0, 8);
+                }
+                o.matId = s->mat.get()[k];
+            }
+        });
+        s->tris = std::move(t);
+    }
+    return s->tris.get();
+}
 
 const char* prt_soup_material_name(const prt_soup* soup, int i)
 {
@@ -634,3 +684,19 @@ const char* prt_soup_material_name(const prt_soup* soup, int i)
 void prt_soup_free(prt_soup* soup) { delete soup; }
 
 } // extern "C"
+
+bool prt_b200::soup_indexed(const prt_soup* s, SoupIndexed* out)
+{
+    if (!s || !out) return false;
+    out->v = s->v.data();
+    out->nv = (long long)s->v.size() / 3;
+    out->vt = s->vt.data();
+    out->nvt = (long long)s->vt.size() / 2;
+    out->vn = s->vn.data();
+    out->nvn = (long long)s->vn.size() / 3;
+    out->corners = s->corners.get();
+    out->cornerInts = s->cornerInts;
+    out->mat = s->mat.get();
+    out->triCount = s->triCount;
+    return true;
+}

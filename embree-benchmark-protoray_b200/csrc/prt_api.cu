@@ -1484,6 +1484,37 @@ int prt_build_mesh(prt_ctx* ctx, const prt_soup_triangle* tris, int triCount, co
     return PRT_OK;
 }
 
+int prt_build_mesh_soup(prt_ctx* ctx, const prt_soup* soup, prt_mesh_info* info)
+{
+    if (!ctx) return PRT_EINVAL;
+    SoupIndexed s;
+    if (!soup_indexed(soup, &s)) return fail(ctx, PRT_EINVAL, "null soup");
+    CK(cudaSetDevice(ctx->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    double buildMs = 0;
+    int st = build_mesh_gpu_indexed(s, ctx->stream, ctx->builtMesh, ctx->err, &buildMs, &ctx->launches);
+    if (st != PRT_OK) return st;
+    const auto t1 = std::chrono::steady_clock::now();
+    BuiltMesh& m = ctx->builtMesh;
+    int names = 0;
+    prt_soup_info(soup, nullptr, &names, nullptr);
+    m.names.clear();
+    for (int i = 0; i < names; ++i) m.names.push_back(prt_soup_material_name(soup, i));
+    if (info)
+    {
+        info->triCount = m.triCount;
+        info->vertCount = m.vertCount;
+        info->hasNormals = m.hasNormals;
+        info->hasTexcoords = m.hasTexcoords;
+        info->hasMaterials = m.hasMaterials;
+        std::memcpy(info->boundsLo, m.lo, sizeof(m.lo));
+        std::memcpy(info->boundsHi, m.hi, sizeof(m.hi));
+        info->buildMs = buildMs;
+        info->totalMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    return PRT_OK;
+}
+
 int prt_read_built_mesh(prt_ctx* ctx, int* indices, int* materialIds, float* positions, float* normals, float* texcoords)
 {
     if (!ctx) return PRT_EINVAL;

@@ -10,6 +10,7 @@
 
 #include "../../include/prt_b200.h"
 #include "prt_device.cuh"
+#include "soup_view.h"
 
 namespace prt_b200 {
 
@@ -112,10 +113,15 @@ struct BuiltMesh
     }
 };
 
-// TriangleMeshBuilder on the device; hostTris may be host or device memory.
-// On success `out` owns the mesh (names are left to the caller).
+// TriangleMeshBuilder on the device; hostTris may be host or device memory
+// (soupOnDevice: device memory the builder may read in place).  On success
+// `out` owns the mesh (names are left to the caller).
 int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream, BuiltMesh& out, std::string& err,
-                   double* buildMs, long long* launches);
+                   double* buildMs, long long* launches, bool soupOnDevice = false);
+// The same for a parsed OBJ soup: uploads its indexed form and expands the
+// triangle records on the device.
+int build_mesh_gpu_indexed(const SoupIndexed& soup, cudaStream_t stream, BuiltMesh& out, std::string& err,
+                           double* buildMs, long long* launches);
 
 // Arguments of one wave of the wavefront renderer.
 struct WaveArgs

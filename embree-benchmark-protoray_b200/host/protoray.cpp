@@ -18,8 +18,9 @@
 //
 //   protoray build input.obj|input.mesh [-o output] [-t mesh] [-threads N]
 //
-// parses the OBJ on host threads and builds the indexed mesh on the GPU
-// (prt_soup_load_obj + prt_build_mesh), then writes the .mesh blob; the output
+// parses the OBJ on host threads and builds the indexed mesh on the GPU from
+// the OBJ's indexed form (prt_soup_load_obj + prt_build_mesh_soup), then
+// writes the .mesh blob; the output
 // defaults to the input name with its extension replaced by the type
 // (build.cpp:84-85).  A .mesh input is read and written back.  Unlike the
 // reference, which ignores ObjLoader::load's result and writes an empty mesh
@@ -425,15 +426,13 @@ int main_build(const std::vector<std::string>& args)
         ~SoupFree() { prt_soup_free(s); }
     } soupFree{soup};
     const auto t1 = std::chrono::steady_clock::now();
-    int triCount = 0, nameCount = 0, degenerate = 0;
-    prt_soup_info(soup, &triCount, &nameCount, &degenerate);
+    int degenerate = 0;
+    prt_soup_info(soup, nullptr, nullptr, &degenerate);
     if (degenerate > 0) say("Removed " + std::to_string(degenerate) + " degenerate triangles");
-    std::vector<const char*> names((size_t)nameCount);
-    for (int i = 0; i < nameCount; ++i) names[(size_t)i] = prt_soup_material_name(soup, i);
 
     DeviceB200 dev(0);
     prt_mesh_info info;
-    int st = prt_build_mesh(dev.handle(), prt_soup_triangles(soup), triCount, names.data(), nameCount, &info);
+    int st = prt_build_mesh_soup(dev.handle(), soup, &info);
     if (st != PRT_OK) throw std::runtime_error(prt_last_error(dev.handle()));
     st = prt_save_built_mesh(dev.handle(), output.c_str());
     if (st != PRT_OK) throw std::runtime_error(prt_last_error(dev.handle()));

@@ -36,7 +36,7 @@ EXPORTS = [
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
     "prt_render_batch", "prt_read_accel", "prt_read_counters", "prt_debug_fail_allocations", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
     "prt_soup_load_obj", "prt_soup_info", "prt_soup_triangles", "prt_soup_material_name", "prt_soup_free",
-    "prt_build_mesh", "prt_read_built_mesh", "prt_save_built_mesh",
+    "prt_build_mesh", "prt_build_mesh_soup", "prt_read_built_mesh", "prt_save_built_mesh",
 ]
 
 
@@ -150,6 +150,7 @@ def lib() -> C.CDLL:
         "prt_soup_material_name": (C.c_char_p, [vp, ip]),
         "prt_soup_free": (None, [vp]),
         "prt_build_mesh": (ip, [vp, vp, ip, C.POINTER(C.c_char_p), ip, C.POINTER(MeshInfo)]),
+        "prt_build_mesh_soup": (ip, [vp, vp, C.POINTER(MeshInfo)]),
         "prt_read_built_mesh": (ip, [vp, vp, vp, vp, vp, vp]),
         "prt_save_built_mesh": (ip, [vp, C.c_char_p]),
     }
@@ -173,27 +174,51 @@ def fail_allocations(after: int) -> None:
     lib().prt_debug_fail_allocations(after)
 
 
+class Soup:
+    """A parsed OBJ (prt_soup_load_obj, ObjLoader::load in the reference)."""
+
+    def __init__(self, path: str, threads: int = 0):
+        self.L = lib()
+        self.h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        st = self.L.prt_soup_load_obj(path.encode(), threads, C.byref(self.h), err, 512)
+        if st != PRT_OK:
+            self.h = None
+            raise PrtError(st, err.value.decode())
+        n, m, d = C.c_int(), C.c_int(), C.c_int()
+        self.L.prt_soup_info(self.h, C.byref(n), C.byref(m), C.byref(d))
+        self.tri_count, self.degenerate = n.value, d.value
+        self.names = [self.L.prt_soup_material_name(self.h, i).decode() for i in range(m.value)]
+
+    def triangles(self) -> np.ndarray:
+        """The expanded soup records as a SOUP_DTYPE array."""
+        tris = np.zeros(self.tri_count, SOUP_DTYPE)
+        if self.tri_count:
+            p = self.L.prt_soup_triangles(self.h)
+            if not p:
+                raise PrtError(PRT_ENOMEM, "prt_soup_triangles")
+            C.memmove(tris.ctypes.data, p, self.tri_count * SOUP_DTYPE.itemsize)
+        return tris
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.prt_soup_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 def load_obj(path: str, threads: int = 0):
     """OBJ -> triangle soup (ObjLoader::load, main/build/obj_loader.cpp:35-53).
 
     Returns (triangles as a SOUP_DTYPE array, material names, dropped
     degenerate triangles); raises PrtError on a malformed file."""
-    L = lib()
-    h = C.c_void_p()
-    err = C.create_string_buffer(512)
-    st = L.prt_soup_load_obj(path.encode(), threads, C.byref(h), err, 512)
-    if st != PRT_OK:
-        raise PrtError(st, err.value.decode())
+    s = Soup(path, threads)
     try:
-        n, m, d = C.c_int(), C.c_int(), C.c_int()
-        L.prt_soup_info(h, C.byref(n), C.byref(m), C.byref(d))
-        tris = np.zeros(n.value, SOUP_DTYPE)
-        if n.value:
-            C.memmove(tris.ctypes.data, L.prt_soup_triangles(h), n.value * SOUP_DTYPE.itemsize)
-        names = [L.prt_soup_material_name(h, i).decode() for i in range(m.value)]
-        return tris, names, d.value
+        return s.triangles(), s.names, s.degenerate
     finally:
-        L.prt_soup_free(h)
+        s.close()
 
 
 def camera_from_view(view, width: int, height: int) -> Camera:
@@ -404,6 +429,16 @@ class Context:
         info = MeshInfo()
         self._check(self.L.prt_build_mesh(self.h, tris.ctypes.data if len(tris) else None, len(tris), arr, len(names),
                                           C.byref(info)), "prt_build_mesh")
+        self._mesh_info = info
+        return {"triCount": info.triCount, "vertCount": info.vertCount, "hasNormals": bool(info.hasNormals),
+                "hasTexcoords": bool(info.hasTexcoords), "hasMaterials": bool(info.hasMaterials),
+                "boundsLo": np.array(info.boundsLo[:], np.float32), "boundsHi": np.array(info.boundsHi[:], np.float32),
+                "buildMs": info.buildMs, "totalMs": info.totalMs}
+
+    def build_mesh_soup(self, soup: "Soup") -> Dict[str, object]:
+        """prt_build_mesh_soup: the GPU builder on a parsed OBJ's indexed form."""
+        info = MeshInfo()
+        self._check(self.L.prt_build_mesh_soup(self.h, soup.h, C.byref(info)), "prt_build_mesh_soup")
         self._mesh_info = info
         return {"triCount": info.triCount, "vertCount": info.vertCount, "hasNormals": bool(info.hasNormals),
                 "hasTexcoords": bool(info.hasTexcoords), "hasMaterials": bool(info.hasMaterials),

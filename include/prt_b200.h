@@ -315,6 +315,12 @@ typedef struct prt_mesh_info {
  * of ctx until the next call; material names are kept with it. */
 int prt_build_mesh(prt_ctx* ctx, const prt_soup_triangle* tris, int triCount, const char* const* materialNames,
                    int materialCount, prt_mesh_info* info);
+/* prt_build_mesh for a soup from prt_soup_load_obj, with the same result as
+ * prt_build_mesh on prt_soup_triangles(soup) and the soup's material names:
+ * uploads the soup's indexed form (the OBJ's vertex lists and each
+ * triangle's corner indices: 12 bytes per triangle plus 12 per vertex for a
+ * positions-only file, instead of 100 per triangle) and expands it on the GPU. */
+int prt_build_mesh_soup(prt_ctx* ctx, const prt_soup* soup, prt_mesh_info* info);
 /* Copies the built mesh to host arrays: indices[3*triCount],
  * materialIds[triCount], positions[3*vertCount]; normals[3*vertCount] and
  * texcoords[2*vertCount] only when present (else pass NULL). */

@@ -272,3 +272,31 @@ def test_cli_build(obj_golden, tmp_path):
         f.write("v 1 2\n")
     r = subprocess.run([exe, "build", bad], cwd=str(tmp_path), capture_output=True, text=True, timeout=120)
     assert r.returncode == 1 and not os.path.exists(str(tmp_path / "bad.mesh"))
+
+
+def test_soup_path_equals_triangle_path(obj_golden, ctx, tmp_path):
+    """prt_build_mesh_soup (indexed upload, expansion on the GPU) writes the
+    same .mesh as prt_build_mesh on the expanded soup, for every accepted
+    OBJ fixture and a larger multi-chunk file."""
+    import prt
+    files = []
+    for i, name in enumerate(obj_golden["obj_names"]):
+        if obj_golden["obj_ok"][i]:
+            p = str(tmp_path / f"{name}.obj")
+            with open(p, "wb") as f:
+                f.write(obj_golden[f"obj_text_{i}"].tobytes())
+            files.append((name, p))
+    p = str(tmp_path / "large.obj")
+    with open(p, "w") as f:
+        f.write(obj_cases.large_obj(seed=13))
+    files.append(("large", p))
+    for name, path in files:
+        soup = prt.Soup(path, 4)
+        a, b = str(tmp_path / f"{name}_soup.mesh"), str(tmp_path / f"{name}_tris.mesh")
+        ctx.build_mesh_soup(soup)
+        ctx.save_built_mesh(a)
+        ctx.build_mesh(soup.triangles(), soup.names)
+        ctx.save_built_mesh(b)
+        soup.close()
+        assert open(a, "rb").read() == open(b, "rb").read(), name
+

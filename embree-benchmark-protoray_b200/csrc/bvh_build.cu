@@ -10,10 +10,10 @@
 //   3. stable LSD radix sort of (code, triangle) pairs, 4-bit digits
 //   4. binary radix tree over the sorted codes (Karras, HPG 2012); equal
 //      codes are ordered by their position, so duplicates are handled
-//   5. bottom-up bounds refit (second child to arrive computes the union)
-//   6. SAH-optimal grouping of the binary nodes into 8-wide nodes (dynamic
-//      program of Ylitie et al. 2017 over the LBVH, bottom-up like the refit)
-//   7. top-down collapse into 8-wide nodes, one tree level per launch:
+//   5. bottom-up bounds refit (second child to arrive computes the union),
+//      fused with the SAH-optimal grouping of the binary nodes into 8-wide
+//      nodes (dynamic program of Ylitie et al. 2017 over the LBVH)
+//   6. top-down collapse into 8-wide nodes, one tree level per launch:
 //      children are the roots chosen by the dynamic program (or, for trees
 //      the program makes deeper than the traversal stack, opened greedily by
 //      largest surface area while fewer than 8 exist); child slots are
@@ -193,51 +193,24 @@ __global__ void k_karras(const uint32_t* __restrict__ keys, int n, int2* __restr
     if (i == 0) parent[0] = -1;
 }
 
-// --- 5. bottom-up refit -----------------------------------------------------
-
-__global__ void k_refit(int n, const uint32_t* __restrict__ vals, const float* __restrict__ triBox,
-                        const int2* __restrict__ child, const int* __restrict__ parent, float* box, int* flag)
-{
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    // leaf box
-    uint32_t p = vals[k];
-    float* lb = box + 6 * (size_t)((n - 1) + k);
-#pragma unroll
-    for (int c = 0; c < 6; ++c) lb[c] = triBox[6 * (size_t)p + c];
-    int node = parent[(n - 1) + k];
-    while (node >= 0)
-    {
-        __threadfence();
-        if (atomicAdd(&flag[node], 1) == 0) return;   // the sibling finishes this node
-        int2 ch = child[node];
-        int a = ch.x >= 0 ? ch.x : (n - 1) + ~ch.x;
-        int b = ch.y >= 0 ? ch.y : (n - 1) + ~ch.y;
-        float r[6];
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-        {
-            r[c] = fminf(__ldcg(box + 6 * (size_t)a + c), __ldcg(box + 6 * (size_t)b + c));
-            r[3 + c] = fmaxf(__ldcg(box + 6 * (size_t)a + 3 + c), __ldcg(box + 6 * (size_t)b + 3 + c));
-        }
-#pragma unroll
-        for (int c = 0; c < 6; ++c) __stcg(box + 6 * (size_t)node + c, r[c]);
-        node = parent[node];
-    }
-}
-
-// --- 5b. SAH-optimal grouping into 8-wide nodes ------------------------------
+// --- 5. bottom-up refit and SAH-optimal grouping into 8-wide nodes ----------
 //
-// Dynamic program of Ylitie, Karras and Laine (HPG 2017, sec. 4.1) over the
-// LBVH: C(u, i), i = 1..8, is the least SAH cost of representing subtree u by
-// at most i roots (children of the enclosing 8-wide node).  A leaf root costs
-// area x cTri x triangles, an 8-wide node area x cNode plus the best split of
-// its 8 slots between the binary children; C(u, i) = min(C(u, i - 1), best
-// split of i slots).  One thread per triangle walks up the tree as in k_refit;
-// the second arrival at a node evaluates it.  dec[8u + i - 1] records the
-// choice: for i = 1 whether u is best a leaf (1) or an 8-wide node (0); for
-// i >= 2 the slots j given to the left child (low 7 bits), with 0x80 set when
-// at most i - 1 roots are no worse.  Costs are relative to cNode = 1.
+// One thread per triangle walks up the tree; the second thread to arrive at
+// a node (atomic counter) computes it from its two finished children, so every
+// node is computed once, after both children.
+//
+// The node box is the union of the children's boxes.  With kGroup the same
+// pass runs the dynamic program of Ylitie, Karras and Laine (HPG 2017,
+// sec. 4.1) over the LBVH: C(u, i), i = 1..8, is the least SAH cost of
+// representing subtree u by at most i roots (children of the enclosing 8-wide
+// node).  A leaf root costs area x cTri x triangles, an 8-wide node area x
+// cNode plus the best split of its 8 slots between the binary children;
+// C(u, i) = min(C(u, i - 1), best split of i slots).  Costs are relative to
+// cNode = 1 and kept for internal nodes only (a single triangle costs its
+// area x cTri for every i).  Byte i - 1 of dec[u] records the choice: for
+// i = 1 whether u is best a leaf (1) or an 8-wide node (0); for i >= 2 the
+// slots j given to the left child (low 7 bits), with 0x80 set when at most
+// i - 1 roots are no worse.
 #ifndef PRT_WIDE_DP
 #define PRT_WIDE_DP 1
 #endif
@@ -251,80 +224,122 @@ __device__ __forceinline__ float box_half_area(const float* b)
     return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_wide_dp(int n, const int2* __restrict__ child, const int2* __restrict__ range,
-                          const int* __restrict__ parent, const float* box, int* flag, float* cost, uint8_t* dec,
-                          int leafMax)
+struct RefitArgs
 {
+    int n;
+    const uint32_t* vals;   // sorted triangle ids
+    const float* triBox;    // 6 floats per triangle, by triangle id
+    const int2* child;
+    const int2* range;
+    const int* parent;
+    float* box;             // 6 floats per node: internal [0, n-1), leaves [n-1, 2n-1)
+    int* flag;              // arrivals per internal node, zeroed
+    float4* cost;           // kGroup: 2 float4 (C(u, 1..8)) per internal node
+    uint2* dec;             // kGroup: 8 decision bytes per internal node
+    int leafMax;
+};
+
+// C(child, 1..8) of a binary child: loaded for an internal node, its area x
+// cTri for a single triangle.
+__device__ __forceinline__ void child_costs(const RefitArgs& a, int ref, const float* b, float* c)
+{
+    if (ref < 0)
+    {
+        const float leafCost = box_half_area(b) * PRT_SAH_CTRI;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) c[i] = leafCost;
+        return;
+    }
+    const float4 lo = __ldcg(a.cost + 2 * (size_t)ref), hi = __ldcg(a.cost + 2 * (size_t)ref + 1);
+    c[0] = lo.x; c[1] = lo.y; c[2] = lo.z; c[3] = lo.w;
+    c[4] = hi.x; c[5] = hi.y; c[6] = hi.z; c[7] = hi.w;
+}
+
+template <bool kGroup>
+__global__ void k_refit(RefitArgs a)
+{
+    const int n = a.n;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const size_t u0 = (size_t)(n - 1) + k;
-    float b6[6];
+    // leaf box
+    uint32_t p = a.vals[k];
+    float* lb = a.box + 6 * (size_t)((n - 1) + k);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) b6[c] = __ldcg(box + 6 * u0 + c);
-    const float leafCost = box_half_area(b6) * PRT_SAH_CTRI;
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-    {
-        __stcg(cost + 8 * u0 + i, leafCost);
-        dec[8 * u0 + i] = i == 0 ? 1 : 0x80;
-    }
-    int node = parent[u0];
+    for (int c = 0; c < 6; ++c) lb[c] = a.triBox[6 * (size_t)p + c];
+    int node = a.parent[(n - 1) + k];
     while (node >= 0)
     {
         __threadfence();
-        if (atomicAdd(&flag[node], 1) == 0) return;   // the sibling finishes this node
-        const int2 ch = child[node];
-        const size_t ua = ch.x >= 0 ? (size_t)ch.x : (size_t)(n - 1) + ~ch.x;
-        const size_t ub = ch.y >= 0 ? (size_t)ch.y : (size_t)(n - 1) + ~ch.y;
-        float ca[8], cb[8];
+        if (atomicAdd(&a.flag[node], 1) == 0) return;   // the sibling finishes this node
+        const int2 ch = a.child[node];
+        const int ia = ch.x >= 0 ? ch.x : (n - 1) + ~ch.x;
+        const int ib = ch.y >= 0 ? ch.y : (n - 1) + ~ch.y;
+        float ba[6], bb[6], r[6];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int c = 0; c < 6; ++c)
         {
-            ca[i] = __ldcg(cost + 8 * ua + i);
-            cb[i] = __ldcg(cost + 8 * ub + i);
+            ba[c] = __ldcg(a.box + 6 * (size_t)ia + c);
+            bb[c] = __ldcg(a.box + 6 * (size_t)ib + c);
         }
 #pragma unroll
-        for (int c = 0; c < 6; ++c) b6[c] = __ldcg(box + 6 * (size_t)node + c);
-        const float area = box_half_area(b6);
-        const int2 rg = range[node];
-        const int cnt = rg.y - rg.x + 1;
-        float dist[8];
-        uint8_t split[8];
-        dist[0] = FLT_MAX;
-        split[0] = 0;
-#pragma unroll
-        for (int i = 2; i <= 8; ++i)
+        for (int c = 0; c < 3; ++c)
         {
-            float best = FLT_MAX;
-            int bj = 1;
+            r[c] = fminf(ba[c], bb[c]);
+            r[3 + c] = fmaxf(ba[3 + c], bb[3 + c]);
+        }
 #pragma unroll
-            for (int j = 1; j < i; ++j)
+        for (int c = 0; c < 6; ++c) __stcg(a.box + 6 * (size_t)node + c, r[c]);
+        if (kGroup)
+        {
+            float ca[8], cb[8];
+            child_costs(a, ch.x, ba, ca);
+            child_costs(a, ch.y, bb, cb);
+            const float area = box_half_area(r);
+            const int2 rg = a.range[node];
+            const int cnt = rg.y - rg.x + 1;
+            float dist[8];
+            uint8_t split[8];
+            dist[0] = FLT_MAX;
+            split[0] = 0;
+#pragma unroll
+            for (int i = 2; i <= 8; ++i)
             {
-                const float v = ca[j - 1] + cb[i - j - 1];
-                if (v < best)
-                {
-                    best = v;
-                    bj = j;
-                }
-            }
-            dist[i - 1] = best;
-            split[i - 1] = (uint8_t)bj;
-        }
-        const float leafOpt = cnt <= leafMax ? area * PRT_SAH_CTRI * (float)cnt : FLT_MAX;
-        const float wideOpt = area + dist[7];
-        float c = fminf(leafOpt, wideOpt);
-        __stcg(cost + 8 * (size_t)node, c);
-        dec[8 * (size_t)node] = leafOpt <= wideOpt ? 1 : 0;
+                float best = FLT_MAX;
+                int bj = 1;
 #pragma unroll
-        for (int i = 2; i <= 8; ++i)
-        {
-            uint8_t d = split[i - 1];
-            if (c <= dist[i - 1]) d |= 0x80;
-            else c = dist[i - 1];
-            __stcg(cost + 8 * (size_t)node + i - 1, c);
-            dec[8 * (size_t)node + i - 1] = d;
+                for (int j = 1; j < i; ++j)
+                {
+                    const float v = ca[j - 1] + cb[i - j - 1];
+                    if (v < best)
+                    {
+                        best = v;
+                        bj = j;
+                    }
+                }
+                dist[i - 1] = best;
+                split[i - 1] = (uint8_t)bj;
+            }
+            const float leafOpt = cnt <= a.leafMax ? area * PRT_SAH_CTRI * (float)cnt : FLT_MAX;
+            const float wideOpt = area + dist[7];
+            float cs[8];
+            float c = fminf(leafOpt, wideOpt);
+            cs[0] = c;
+            uint32_t d0 = leafOpt <= wideOpt ? 1u : 0u, d1 = 0;
+#pragma unroll
+            for (int i = 2; i <= 8; ++i)
+            {
+                uint32_t d = split[i - 1];
+                if (c <= dist[i - 1]) d |= 0x80;
+                else c = dist[i - 1];
+                cs[i - 1] = c;
+                if (i <= 4) d0 |= d << (8 * (i - 1));
+                else d1 |= d << (8 * (i - 5));
+            }
+            __stcg(a.cost + 2 * (size_t)node, make_float4(cs[0], cs[1], cs[2], cs[3]));
+            __stcg(a.cost + 2 * (size_t)node + 1, make_float4(cs[4], cs[5], cs[6], cs[7]));
+            __stcg(a.dec + node, make_uint2(d0, d1));
         }
-        node = parent[node];
+        node = a.parent[node];
     }
 }
 
@@ -346,7 +361,7 @@ struct CollapseArgs
     int nodeCapacity;
     int* error;
     int leafMax;   // subtrees of at most this many triangles (1..3) become leaves
-    const uint8_t* dec;   // decisions of k_wide_dp, or nullptr for the greedy grouping
+    const uint8_t* dec;   // grouping decisions of k_refit<true>, or nullptr for the greedy grouping
 };
 
 __device__ __forceinline__ int ref_count(const CollapseArgs& a, int ref)
@@ -395,7 +410,7 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
     }
     else if (a.dec)
     {
-        // the roots of the best split of 8 slots (k_wide_dp decisions)
+        // the roots of the best split of 8 slots (grouping decisions)
         int2 st[16];
         int sp = 0;
         const int2 c = a.child[bref];
@@ -656,6 +671,22 @@ int collapse_levels(const CollapseArgs& a, int2* workA, int2* workB, int* counte
         }                                                                                                      \
     } while (0)
 
+// Scratch buffers of one build, carved from one allocation (each 256-byte
+// aligned): a dry run with a null base measures the block.
+struct Carve
+{
+    char* base;
+    size_t off = 0;
+    template <class T>
+    T* take(size_t count)
+    {
+        off = (off + 255) & ~(size_t)255;
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += sizeof(T) * count;
+        return p;
+    }
+};
+
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
                std::string& err, BuildInfo* info, int leafMax, bool sahGrouping)
 {
@@ -669,16 +700,38 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     const size_t histCount = radix_sort_hist_entries(n);
     const int boundBlocks = std::min(1024, div_up(n, 256));
     const int nodeCapacity = std::max(1, nInternal);
+    const bool group = PRT_WIDE_DP && sahGrouping && nInternal > 0;
 
-    float* triBox = nullptr;
-    float* partial = nullptr;
-    float* cbounds = nullptr;
-    uint32_t *keysA = nullptr, *keysB = nullptr, *valsA = nullptr, *valsB = nullptr, *hist = nullptr;
-    int2 *child = nullptr, *range = nullptr, *workA = nullptr, *workB = nullptr;
-    int *parent = nullptr, *flag = nullptr, *counters = nullptr;
-    float* box = nullptr;
-    float* dpCost = nullptr;
-    uint8_t* dpDec = nullptr;
+    char* block = nullptr;
+    float *triBox, *partial, *cbounds, *box;
+    uint32_t *keysA, *keysB, *valsA, *valsB, *hist;
+    int2 *child, *range, *workA, *workB;
+    int *parent, *flag, *counters;
+    float4* dpCost;
+    uint2* dpDec;
+    auto carve = [&](char* base) {
+        Carve c{base};
+        triBox = c.take<float>(6 * (size_t)n);
+        partial = c.take<float>(6 * (size_t)boundBlocks);
+        cbounds = c.take<float>(6);
+        keysA = c.take<uint32_t>(n);
+        keysB = c.take<uint32_t>(n);
+        valsA = c.take<uint32_t>(n);
+        valsB = c.take<uint32_t>(n);
+        hist = c.take<uint32_t>(histCount);
+        child = c.take<int2>(nodeCapacity);
+        range = c.take<int2>(nodeCapacity);
+        parent = c.take<int>(2 * (size_t)n);
+        flag = c.take<int>(nodeCapacity);
+        box = c.take<float>(6 * (size_t)(2 * n));
+        workA = c.take<int2>(nodeCapacity);
+        workB = c.take<int2>(nodeCapacity);
+        counters = c.take<int>(4);
+        dpCost = group ? c.take<float4>(2 * (size_t)nodeCapacity) : nullptr;
+        dpDec = group ? c.take<uint2>(nodeCapacity) : nullptr;
+        return c.off;
+    };
+    const size_t scratchBytes = carve(nullptr);
     int levels = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -686,22 +739,8 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     BUILD_CHECK(cudaEventCreate(&ev1));
     BUILD_CHECK(cudaEventRecord(ev0, stream));
 
-    BUILD_CHECK(dev_malloc(&triBox, sizeof(float) * 6 * (size_t)n));
-    BUILD_CHECK(dev_malloc(&partial, sizeof(float) * 6 * (size_t)boundBlocks));
-    BUILD_CHECK(dev_malloc(&cbounds, sizeof(float) * 6));
-    BUILD_CHECK(dev_malloc(&keysA, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(dev_malloc(&keysB, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(dev_malloc(&valsA, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(dev_malloc(&valsB, sizeof(uint32_t) * (size_t)n));
-    BUILD_CHECK(dev_malloc(&hist, sizeof(uint32_t) * (size_t)histCount));
-    BUILD_CHECK(dev_malloc(&child, sizeof(int2) * (size_t)std::max(1, nInternal)));
-    BUILD_CHECK(dev_malloc(&range, sizeof(int2) * (size_t)std::max(1, nInternal)));
-    BUILD_CHECK(dev_malloc(&parent, sizeof(int) * (size_t)(2 * n)));
-    BUILD_CHECK(dev_malloc(&flag, sizeof(int) * (size_t)std::max(1, nInternal)));
-    BUILD_CHECK(dev_malloc(&box, sizeof(float) * 6 * (size_t)(2 * n)));
-    BUILD_CHECK(dev_malloc(&workA, sizeof(int2) * (size_t)nodeCapacity));
-    BUILD_CHECK(dev_malloc(&workB, sizeof(int2) * (size_t)nodeCapacity));
-    BUILD_CHECK(dev_malloc(&counters, sizeof(int) * 4));
+    BUILD_CHECK(dev_malloc(&block, scratchBytes));
+    carve(block);
     {
         const size_t nodeBytes = (sizeof(Bvh8Node) * (size_t)nodeCapacity + 255) & ~(size_t)255;
         out.bytes = nodeBytes + sizeof(TriRec) * (size_t)n;
@@ -726,18 +765,23 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         int minus1 = -1;
         BUILD_CHECK(cudaMemcpyAsync(parent, &minus1, sizeof(int), cudaMemcpyHostToDevice, stream));
     }
-    k_refit<<<div_up(n, 256), 256, 0, stream>>>(n, valsA, triBox, child, parent, box, flag);
-    BUILD_CHECK(cudaGetLastError());
-
-    if (PRT_WIDE_DP && sahGrouping && nInternal > 0)
     {
-        BUILD_CHECK(dev_malloc(&dpCost, sizeof(float) * 8 * (size_t)(2 * n)));
-        BUILD_CHECK(dev_malloc(&dpDec, sizeof(uint8_t) * 8 * (size_t)(2 * n)));
-        BUILD_CHECK(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)nInternal, stream));
-        k_wide_dp<<<div_up(n, 256), 256, 0, stream>>>(n, child, range, parent, box, flag, dpCost, dpDec,
-                                                     std::max(1, std::min(3, leafMax)));
-        BUILD_CHECK(cudaGetLastError());
+        RefitArgs ra;
+        ra.n = n;
+        ra.vals = valsA;
+        ra.triBox = triBox;
+        ra.child = child;
+        ra.range = range;
+        ra.parent = parent;
+        ra.box = box;
+        ra.flag = flag;
+        ra.cost = dpCost;
+        ra.dec = dpDec;
+        ra.leafMax = std::max(1, std::min(3, leafMax));
+        if (group) k_refit<true><<<div_up(n, 256), 256, 0, stream>>>(ra);
+        else k_refit<false><<<div_up(n, 256), 256, 0, stream>>>(ra);
     }
+    BUILD_CHECK(cudaGetLastError());
 
     {
         CollapseArgs a;
@@ -755,7 +799,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         a.nodeCapacity = nodeCapacity;
         a.error = counters + 3;
         a.leafMax = std::max(1, std::min(3, leafMax));
-        a.dec = dpDec;
+        a.dec = reinterpret_cast<const uint8_t*>(dpDec);
         int nodeCount = 0, triCount = 0;
         status = collapse_levels(a, workA, workB, counters, n, stream, nodeCount, triCount, levels, err);
         if (status == PRT_OK && a.dec && 2 * levels > kStackMax)
@@ -795,24 +839,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     }
 
 done:
-    cudaFree(triBox);
-    cudaFree(partial);
-    cudaFree(cbounds);
-    cudaFree(keysA);
-    cudaFree(keysB);
-    cudaFree(valsA);
-    cudaFree(valsB);
-    cudaFree(hist);
-    cudaFree(child);
-    cudaFree(range);
-    cudaFree(parent);
-    cudaFree(flag);
-    cudaFree(box);
-    cudaFree(dpCost);
-    cudaFree(dpDec);
-    cudaFree(workA);
-    cudaFree(workB);
-    cudaFree(counters);
+    cudaFree(block);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (status != PRT_OK) out.release();

@@ -13,7 +13,8 @@
 //   5. bottom-up bounds refit (second child to arrive computes the union),
 //      fused with the SAH-optimal grouping of the binary nodes into 8-wide
 //      nodes (dynamic program of Ylitie et al. 2017 over the LBVH)
-//   6. top-down collapse into 8-wide nodes, one tree level per launch:
+//   6. top-down collapse into 8-wide nodes, one tree level per launch (no
+//      host round trip between levels), one 8-lane group per node:
 //      children are the roots chosen by the dynamic program (or, for trees
 //      the program makes deeper than the traversal stack, opened greedily by
 //      largest surface area while fewer than 8 exist); child slots are
@@ -360,24 +361,23 @@ struct CollapseArgs
     int* triCounter;
     int nodeCapacity;
     int* error;
-    int leafMax;   // subtrees of at most this many triangles (1..3) become leaves
-    const uint8_t* dec;   // grouping decisions of k_refit<true>, or nullptr for the greedy grouping
+    int leafMax;          // subtrees of at most this many triangles (1..3) become leaves
+    const uint2* dec;     // grouping decisions of k_refit<true>, or nullptr for the greedy grouping
+    int* counts;          // work items per level: counts[l] items of level l, kCollapseLevels + 1 entries
+    int2* work[2];        // work items of even / odd levels
 };
+
+// Levels launched; a tree that needs more would overflow the traversal stack
+// (two entries per level) and is rejected.
+constexpr int kCollapseLevels = kStackMax / 2;
+constexpr int kCollapseBlock = 128;
+constexpr int kGroupsPerBlock = kCollapseBlock / 8;
 
 __device__ __forceinline__ int ref_count(const CollapseArgs& a, int ref)
 {
     if (ref < 0) return 1;
     int2 r = a.range[ref];
     return r.y - r.x + 1;
-}
-
-// A child of an 8-wide node is a leaf (its triangles) or an 8-wide node.
-__device__ __forceinline__ bool ref_is_leaf(const CollapseArgs& a, int ref)
-{
-    if (ref < 0) return true;
-    int2 r = a.range[ref];
-    if (r.y - r.x + 1 > a.leafMax) return false;
-    return a.dec ? a.dec[8 * (size_t)ref] == 1 : true;
 }
 
 __device__ __forceinline__ const float* ref_box(const CollapseArgs& a, int ref)
@@ -391,139 +391,280 @@ __device__ __forceinline__ float half_area(const float* b)
     return dx * dy + dy * dz + dz * dx;
 }
 
+__device__ __forceinline__ uint32_t dec_byte(uint2 d, int b)
+{
+    return ((b < 4 ? d.x : d.y) >> (8 * (b & 3))) & 0xffu;
+}
+
+// Per-group shared staging: the node being written (80 bytes), the children's
+// slot records and the work list of the grouping walk.
+struct __align__(16) CollapseGroup
+{
+    uint8_t node[80];
+    uint32_t slotRec[8];   // per slot: bit 31 occupied, bit 30 internal, low bits triangle count
+    int2 front[8];
+};
+
+// One 8-lane group builds one 8-wide node: lane c holds child c of the node.
 // Work item: (binary reference, 8-wide node index).  A binary reference of
 // ~0 with n == 1 is the single-triangle scene.
-__global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int workCount, int2* __restrict__ next,
-                           int* __restrict__ nextCount)
+__device__ void collapse_node(const CollapseArgs& a, int2 item, int level, int sub, unsigned gmask,
+                              CollapseGroup& g)
 {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= workCount) return;
-    int bref = work[w].x;
-    int nodeIdx = work[w].y;
+    const int bref = item.x;
+    const int nodeIdx = item.y;
 
-    int ch[8];
-    int nc;
+    // 1. children: the roots chosen by the grouping decisions (or greedily
+    //    opened), left to right in tree order, child c in lane c
+    int r = 0, nc;
     if (bref < 0)
     {
-        ch[0] = bref;
+        r = bref;
         nc = 1;
     }
     else if (a.dec)
     {
-        // the roots of the best split of 8 slots (grouping decisions)
-        int2 st[16];
-        int sp = 0;
+        // expand the split list breadth-first: an entry (u, i) gives i slots
+        // to subtree u; it is final for a triangle or i = 1, else the largest
+        // i' <= i without the "no worse with fewer" bit splits it between the
+        // binary children (i' = 1: u itself is the root)
         const int2 c = a.child[bref];
-        const int j = a.dec[8 * (size_t)bref + 7] & 0x7f;
-        st[sp++] = make_int2(c.y, 8 - j);
-        st[sp++] = make_int2(c.x, j);
-        nc = 0;
-        while (sp > 0 && nc < 8)
+        const int j = (int)(dec_byte(__ldg(a.dec + bref), 7) & 0x7f);
+        r = sub == 0 ? c.x : c.y;
+        int ri = sub == 0 ? j : 8 - j;
+        nc = 2;
+        for (int round = 0; round < 8; ++round)
         {
-            const int2 e = st[--sp];
-            const int r = e.x, i = e.y;
-            if (r < 0 || i <= 1)
+            const bool valid = sub < nc;
+            const bool expand = valid && r >= 0 && ri > 1;
+            uint2 d = make_uint2(0, 0);
+            int2 cc = make_int2(0, 0);
+            if (expand)
             {
-                ch[nc++] = r;
-                continue;
+                d = __ldg(a.dec + r);
+                cc = a.child[r];
             }
-            const uint8_t d = a.dec[8 * (size_t)r + i - 1];
-            if (d & 0x80)
+            int ii = ri;
+            if (expand)
+                while (ii > 1 && (dec_byte(d, ii - 1) & 0x80)) --ii;
+            const bool split = expand && ii > 1;
+            const unsigned splitMask = (__ballot_sync(gmask, split) & gmask) >> (__ffs(gmask) - 1);
+            if (!splitMask) break;
+            if (nc + __popc(splitMask) > 8)
             {
-                st[sp++] = make_int2(r, i - 1);
+                // slot counts that do not add up to 8: inconsistent decisions
+                if (sub == 0) atomicExch(a.error, 1);
+                return;
             }
-            else
+            const int at = min(sub, nc) + __popc(splitMask & ((1u << sub) - 1));
+            if (split)
             {
-                const int2 c2 = a.child[r];
-                st[sp++] = make_int2(c2.y, i - (int)d);
-                st[sp++] = make_int2(c2.x, (int)d);
+                const int dj = (int)dec_byte(d, ii - 1);
+                g.front[at] = make_int2(cc.x, dj);
+                g.front[at + 1] = make_int2(cc.y, ii - dj);
             }
+            else if (valid)
+            {
+                g.front[at] = make_int2(r, expand ? 1 : ri);
+            }
+            nc += __popc(splitMask);
+            __syncwarp(gmask);
+            if (sub < nc)
+            {
+                r = g.front[sub].x;
+                ri = g.front[sub].y;
+            }
+            __syncwarp(gmask);
         }
     }
     else
     {
-        int2 c = a.child[bref];
-        ch[0] = c.x;
-        ch[1] = c.y;
+        // greedy: open the child of largest surface area while fewer than 8
+        // (ties to the lower child); the opened child keeps its left half in
+        // its lane and the right half goes to lane nc
+        const int2 c = a.child[bref];
+        r = sub == 0 ? c.x : c.y;
         nc = 2;
+        bool stale = true;
+        uint32_t key = 0;
         while (nc < 8)
         {
-            int best = -1;
-            float bestA = -1.f;
-            for (int i = 0; i < nc; ++i)
+            if (stale)
             {
-                if (ch[i] < 0 || ref_count(a, ch[i]) <= a.leafMax) continue;
-                float ar = half_area(ref_box(a, ch[i]));
-                if (ar > bestA) { bestA = ar; best = i; }
+                key = 0;
+                if (sub < nc && r >= 0 && ref_count(a, r) > a.leafMax)
+                {
+                    const float ar = half_area(ref_box(a, r));
+                    if (ar >= 0.f) key = ((__float_as_uint(ar) | 0x80000000u) & ~7u) | (uint32_t)(7 - sub);
+                }
+                stale = false;
             }
-            if (best < 0) break;
-            int2 c2 = a.child[ch[best]];
-            ch[best] = c2.x;
-            ch[nc++] = c2.y;
+            const uint32_t top = __reduce_max_sync(gmask, key);
+            if (!top) break;
+            const int best = 7 - (int)(top & 7u);
+            int2 c2 = make_int2(0, 0);
+            if (sub == best) c2 = a.child[r];
+            const int right = __shfl_sync(gmask, c2.y, best, 8);
+            if (sub == best)
+            {
+                r = c2.x;
+                stale = true;
+            }
+            if (sub == nc)
+            {
+                r = right;
+                stale = true;
+            }
+            ++nc;
         }
     }
 
-    // node box = union of child boxes
-    float nb[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
-    float cen[8][3];
-    for (int i = 0; i < nc; ++i)
+    // 2. this lane's child: triangle count, leaf or 8-wide node, box
+    const bool valid = sub < nc;
+    int cnt = 0, first = 0;
+    bool leaf = false;
+    float b[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    if (valid)
     {
-        const float* b = ref_box(a, ch[i]);
+        if (r < 0)
+        {
+            cnt = 1;
+            first = ~r;
+            leaf = true;
+        }
+        else
+        {
+            const int2 rg = a.range[r];
+            cnt = rg.y - rg.x + 1;
+            first = rg.x;
+            leaf = cnt <= a.leafMax && (a.dec ? dec_byte(__ldg(a.dec + r), 0) == 1 : true);
+        }
+        const float* rb = ref_box(a, r);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) b[k] = rb[k];
+    }
+
+    // 3. node box: union over the group
+    float nb[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) nb[k] = b[k];
+#pragma unroll
+    for (int off = 1; off < 8; off <<= 1)
+    {
+#pragma unroll
         for (int k = 0; k < 3; ++k)
         {
-            nb[k] = fminf(nb[k], b[k]);
-            nb[3 + k] = fmaxf(nb[3 + k], b[3 + k]);
-            cen[i][k] = 0.5f * (b[k] + b[3 + k]);
+            nb[k] = fminf(nb[k], __shfl_xor_sync(gmask, nb[k], off, 8));
+            nb[3 + k] = fmaxf(nb[3 + k], __shfl_xor_sync(gmask, nb[3 + k], off, 8));
         }
     }
 
-    // slot assignment: greedy on cost(slot s, child c) = projection of the
-    // child centroid on the direction of octant s (smaller = nearer)
-    int slotOf[8];
-    int childInSlot[8];
-    for (int s = 0; s < 8; ++s) childInSlot[s] = -1;
-    for (int i = 0; i < nc; ++i) slotOf[i] = -1;
-    for (int it = 0; it < nc; ++it)
+    // 4. slot assignment: greedy on cost(slot s, child c) = projection of the
+    //    child centroid on the direction of octant s (smaller = nearer); each
+    //    round places the least cost over free slots and unplaced children,
+    //    ties to the lower slot, then the lower child
+    float cost[8];
     {
-        float bestC = FLT_MAX;
-        int bs = -1, bc = -1;
+        const float cx = 0.5f * (b[0] + b[3]), cy = 0.5f * (b[1] + b[4]), cz = 0.5f * (b[2] + b[5]);
+#pragma unroll
         for (int s = 0; s < 8; ++s)
         {
-            if (childInSlot[s] >= 0) continue;
-            float dx = (s & 1) ? -1.f : 1.f, dy = (s & 2) ? -1.f : 1.f, dz = (s & 4) ? -1.f : 1.f;
-            for (int i = 0; i < nc; ++i)
+            const float dx = (s & 1) ? -1.f : 1.f, dy = (s & 2) ? -1.f : 1.f, dz = (s & 4) ? -1.f : 1.f;
+            cost[s] = cx * dx + cy * dy + cz * dz;
+        }
+    }
+    int slot = -1;
+    unsigned freeSlots = 0xffu;
+    for (int it = 0; it < nc; ++it)
+    {
+        // key: cost (order-preserving bits, 6 low bits dropped), slot, lane;
+        // least wins
+        uint32_t key = 0xffffffffu;
+        if (valid && slot < 0)
+        {
+            float bc = FLT_MAX;
+            int bs = 8;
+#pragma unroll
+            for (int s = 0; s < 8; ++s)
+                if (((freeSlots >> s) & 1u) && cost[s] < bc)
+                {
+                    bc = cost[s];
+                    bs = s;
+                }
+            if (bs < 8)
             {
-                if (slotOf[i] >= 0) continue;
-                float c = cen[i][0] * dx + cen[i][1] * dy + cen[i][2] * dz;
-                if (c < bestC) { bestC = c; bs = s; bc = i; }
+                const uint32_t u = __float_as_uint(bc);
+                const uint32_t ord = u ^ ((uint32_t)((int)u >> 31) | 0x80000000u);
+                key = (ord & ~63u) | ((uint32_t)bs << 3) | (uint32_t)sub;
             }
         }
-        childInSlot[bs] = bc;
-        slotOf[bc] = bs;
+        const uint32_t least = __reduce_min_sync(gmask, key);
+        int bs, bl;
+        if (least != 0xffffffffu)
+        {
+            bs = (int)((least >> 3) & 7u);
+            bl = (int)(least & 7u);
+        }
+        else
+        {
+            // no finite cost left (degenerate boxes): lowest free slot to the
+            // lowest unplaced child
+            bs = __ffs(freeSlots) - 1;
+            const unsigned unplaced = __ballot_sync(gmask, valid && slot < 0) & gmask;
+            bl = __ffs(unplaced >> (__ffs(gmask) - 1)) - 1;
+        }
+        if (sub == bl) slot = bs;
+        freeSlots &= ~(1u << bs);
     }
 
-    // allocate internal children (in slot order) and leaf triangles
-    int nInternal = 0, nTris = 0;
-    for (int i = 0; i < nc; ++i)
+    // 5. per-slot records: internal children numbered and leaf triangles
+    //    packed in slot order
+    if (valid) g.slotRec[slot] = 0x80000000u | (leaf ? 0u : 0x40000000u) | (uint32_t)cnt;
+    if ((freeSlots >> sub) & 1u) g.slotRec[sub] = 0;   // the empty slots
+    __syncwarp(gmask);
+    int nInternal = 0, nTris = 0, internalRank = 0, triOff = 0;
+    uint32_t imask = 0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
     {
-        if (ref_is_leaf(a, ch[i])) nTris += ref_count(a, ch[i]);
-        else nInternal++;
+        const uint32_t rec = g.slotRec[s];
+        if (!(rec & 0x80000000u)) continue;
+        if (rec & 0x40000000u)
+        {
+            if (s < slot) ++internalRank;
+            ++nInternal;
+            imask |= 1u << s;
+        }
+        else
+        {
+            const int c = (int)(rec & 0xffffu);
+            if (s < slot) triOff += c;
+            nTris += c;
+        }
     }
-    int childBase = nInternal ? atomicAdd(a.nodeCounter, nInternal) : 0;
-    int triBase = nTris ? atomicAdd(a.triCounter, nTris) : 0;
-    if (childBase + nInternal > a.nodeCapacity)
+    int childBase = 0, triBase = 0, nextBase = 0, bad = 0;
+    if (sub == 0)
     {
-        atomicExch(a.error, 1);
-        return;
+        childBase = nInternal ? atomicAdd(a.nodeCounter, nInternal) : 0;
+        triBase = nTris ? atomicAdd(a.triCounter, nTris) : 0;
+        bad = childBase + nInternal > a.nodeCapacity || triBase + nTris > a.n;
+        if (bad) atomicExch(a.error, 1);
+        else if (nInternal) nextBase = atomicAdd(a.counts + level + 1, nInternal);
     }
+    const int leader = __ffs(gmask) - 1;
+    if (__shfl_sync(gmask, bad, leader)) return;   // group-uniform
+    childBase = __shfl_sync(gmask, childBase, leader);
+    triBase = __shfl_sync(gmask, triBase, leader);
+    nextBase = __shfl_sync(gmask, nextBase, leader);
 
-    // header: per-axis power-of-two scale s with the node box spanning at most
-    // 253 steps, and origin one step below the box, so every quantized plane
-    // lies at least 2^-8 of a step outside the child box it bounds (the
-    // traversal's plane decode may move a plane inwards by up to 2^-9 step)
+    // 6. header: per-axis power-of-two scale s with the node box spanning at
+    //    most 253 steps, and origin one step below the box, so every quantized
+    //    plane lies at least 2^-8 of a step outside the child box it bounds (the
+    //    traversal's plane decode may move a plane inwards by up to 2^-9 step)
     uint32_t ebits[3];
     float scale[3];
     float origin[3];
+#pragma unroll
     for (int k = 0; k < 3; ++k)
     {
         float ext = nb[3 + k] - nb[k];
@@ -552,108 +693,138 @@ __global__ void k_collapse(CollapseArgs a, const int2* __restrict__ work, int wo
         if ((double)of > o) of = nextafterf(of, -FLT_MAX);
         origin[k] = of;
     }
-    uint8_t meta[8], qlo[3][8], qhi[3][8];
-    uint32_t imask = 0;
-    int internalRank = 0, triOff = 0;
-    for (int s = 0; s < 8; ++s)
+
+    // 7. this lane's slot: quantized planes and meta byte; the lane numbered
+    //    by an empty slot fills in an empty box
+    if ((freeSlots >> sub) & 1u)
     {
-        int i = childInSlot[s];
-        if (i < 0)
-        {
-            meta[s] = 0;
-            for (int k = 0; k < 3; ++k) { qlo[k][s] = 255; qhi[k][s] = 0; }
-            continue;
-        }
-        const float* b = ref_box(a, ch[i]);
+        g.node[24 + sub] = 0;
+#pragma unroll
         for (int k = 0; k < 3; ++k)
         {
-            double lo = floor(((double)b[k] - (double)origin[k]) / (double)scale[k] - 1.0 / 256.0);
-            double hi = ceil(((double)b[3 + k] - (double)origin[k]) / (double)scale[k] + 1.0 / 256.0);
-            qlo[k][s] = (uint8_t)fmax(0.0, fmin(255.0, lo));
-            qhi[k][s] = (uint8_t)fmax(0.0, fmin(255.0, hi));
+            g.node[32 + 8 * k + sub] = 255;
+            g.node[56 + 8 * k + sub] = 0;
         }
-        int cnt = ref_count(a, ch[i]);
-        if (!ref_is_leaf(a, ch[i]))
+    }
+    if (valid)
+    {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
         {
-            meta[s] = (uint8_t)(0x20 | (24 + s));
-            imask |= 1u << s;
-            int2 item = make_int2(ch[i], childBase + internalRank);
-            internalRank++;
-            int slotQ = atomicAdd(nextCount, 1);
-            next[slotQ] = item;
+            // scale is a power of two: multiplying by its inverse is exact
+            const double inv = __longlong_as_double((long long)(127 - (int)ebits[k] + 1023) << 52);
+            double lo = floor(((double)b[k] - (double)origin[k]) * inv - 1.0 / 256.0);
+            double hi = ceil(((double)b[3 + k] - (double)origin[k]) * inv + 1.0 / 256.0);
+            g.node[32 + 8 * k + slot] = (uint8_t)fmax(0.0, fmin(255.0, lo));
+            g.node[56 + 8 * k + slot] = (uint8_t)fmax(0.0, fmin(255.0, hi));
+        }
+        if (!leaf)
+        {
+            g.node[24 + slot] = (uint8_t)(0x20 | (24 + slot));
+            a.work[(level + 1) & 1][nextBase + internalRank] = make_int2(r, childBase + internalRank);
         }
         else
         {
-            uint32_t unary = (1u << cnt) - 1u;
-            meta[s] = (uint8_t)((unary << 5) | (uint32_t)triOff);
-            // copy the triangles of the leaf (a contiguous sorted range)
-            int first = ch[i] < 0 ? ~ch[i] : a.range[ch[i]].x;
+            const uint32_t unary = (1u << cnt) - 1u;
+            g.node[24 + slot] = (uint8_t)((unary << 5) | (uint32_t)triOff);
+            // the triangles of the leaf (a contiguous sorted range)
             for (int k = 0; k < cnt; ++k)
             {
-                uint32_t prim = a.vals[first + k];
-                int i0 = a.idx[3 * prim], i1 = a.idx[3 * prim + 1], i2 = a.idx[3 * prim + 2];
+                const uint32_t prim = a.vals[first + k];
+                const int i0 = a.idx[3 * prim], i1 = a.idx[3 * prim + 1], i2 = a.idx[3 * prim + 2];
                 TriRec tr;
                 tr.v0 = make_float4(a.pos[3 * i0], a.pos[3 * i0 + 1], a.pos[3 * i0 + 2], __int_as_float((int)prim));
                 tr.v1 = make_float4(a.pos[3 * i1], a.pos[3 * i1 + 1], a.pos[3 * i1 + 2], 0.f);
                 tr.v2 = make_float4(a.pos[3 * i2], a.pos[3 * i2 + 1], a.pos[3 * i2 + 2], 0.f);
                 a.tris[triBase + triOff + k] = tr;
             }
-            triOff += cnt;
         }
     }
-    auto pack4 = [](const uint8_t* v) {
-        return (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
-    };
-    Bvh8Node node;
-    node.q[0] = make_uint4(__float_as_uint(origin[0]), __float_as_uint(origin[1]), __float_as_uint(origin[2]),
-                           ebits[0] | (ebits[1] << 8) | (ebits[2] << 16) | (imask << 24));
-    node.q[1] = make_uint4((uint32_t)childBase, (uint32_t)triBase, pack4(meta), pack4(meta + 4));
-    node.q[2] = make_uint4(pack4(qlo[0]), pack4(qlo[0] + 4), pack4(qlo[1]), pack4(qlo[1] + 4));
-    node.q[3] = make_uint4(pack4(qlo[2]), pack4(qlo[2] + 4), pack4(qhi[0]), pack4(qhi[0] + 4));
-    node.q[4] = make_uint4(pack4(qhi[1]), pack4(qhi[1] + 4), pack4(qhi[2]), pack4(qhi[2] + 4));
-    a.nodes[nodeIdx] = node;
+    if (sub == 0)
+    {
+        uint32_t* w = reinterpret_cast<uint32_t*>(g.node);
+        w[0] = __float_as_uint(origin[0]);
+        w[1] = __float_as_uint(origin[1]);
+        w[2] = __float_as_uint(origin[2]);
+        w[3] = ebits[0] | (ebits[1] << 8) | (ebits[2] << 16) | (imask << 24);
+        w[4] = (uint32_t)childBase;
+        w[5] = (uint32_t)triBase;
+    }
+    __syncwarp(gmask);
+    if (sub < 5) a.nodes[nodeIdx].q[sub] = reinterpret_cast<const uint4*>(g.node)[sub];
+    __syncwarp(gmask);
+}
+
+// One tree level: the items of counts[level], one per 8-lane group, grid-strided.
+__global__ void __launch_bounds__(kCollapseBlock) k_collapse(CollapseArgs a, int level)
+{
+    __shared__ CollapseGroup groups[kGroupsPerBlock];
+    if (*(volatile int*)a.error) return;
+    const int count = *(volatile int*)(a.counts + level);
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & 7;
+    const unsigned gmask = 0xffu << (lane & 24);
+    CollapseGroup& g = groups[threadIdx.x >> 3];
+    const int2* work = a.work[level & 1];
+    const int stride = gridDim.x * kGroupsPerBlock;
+    for (int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 3); w < count; w += stride)
+        collapse_node(a, work[w], level, sub, gmask, g);
 }
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// Runs the collapse one level per launch from the root; on success sets the
-// node and triangle counts and the number of 8-wide levels.
-int collapse_levels(const CollapseArgs& a, int2* workA, int2* workB, int* counters, int n, cudaStream_t stream,
+// Runs the collapse from the root, one launch per level, without waiting for
+// the host between levels: launches past the last level find no items and
+// return.  The counters are read back after the first kCollapseBatch levels
+// and, for a deeper tree, after the rest.  On success sets the node and
+// triangle counts and the number of 8-wide levels (kCollapseLevels + 1 for a
+// tree deeper than the launches).
+constexpr int kCollapseBatch = 16;
+
+int collapse_levels(const CollapseArgs& a, int* counters, int n, int numSMs, cudaStream_t stream,
                     int& nodeCount, int& triCount, int& levels, std::string& err)
 {
     int2 root = make_int2(n > 1 ? 0 : ~0, 0);
-    int init[4] = {1, 0, 0, 0};   // nodeCounter, triCounter, nextCount, error
-    int hostCounters[4];
-    cudaError_t e = cudaMemcpyAsync(workA, &root, sizeof(int2), cudaMemcpyHostToDevice, stream);
+    int init[4] = {1, 0, 0, 0};   // nodeCounter, triCounter, unused, error
+    int host[4 + kCollapseLevels + 1];
+    cudaError_t e = cudaMemcpyAsync(a.work[0], &root, sizeof(int2), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream);
-    levels = 0;
-    int workCount = 1;
-    while (e == cudaSuccess && workCount > 0)
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.counts, 0, sizeof(int) * (kCollapseLevels + 1), stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a.counts, &init[0], sizeof(int), cudaMemcpyHostToDevice, stream);
+    const long long maxBlocks = (long long)std::max(1, numSMs) * 8;
+    long long bound = 1;   // level l holds at most 8^l items
+    int l = 0;
+    while (e == cudaSuccess && l < kCollapseLevels)
     {
-        e = cudaMemsetAsync(counters + 2, 0, sizeof(int), stream);
-        if (e != cudaSuccess) break;
-        k_collapse<<<div_up(workCount, 128), 128, 0, stream>>>(a, workA, workCount, workB, counters + 2);
-        e = cudaGetLastError();
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(hostCounters, counters, sizeof(hostCounters), cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) break;
-        ++levels;
-        if (hostCounters[3])
+        const int end = std::min(kCollapseLevels, l + kCollapseBatch);
+        for (; e == cudaSuccess && l < end; ++l)
         {
-            err = "BVH8 collapse exceeded its node capacity";
-            return PRT_EINTERNAL;
+            const int blocks = (int)std::min(maxBlocks, (bound + kGroupsPerBlock - 1) / kGroupsPerBlock);
+            k_collapse<<<blocks, kCollapseBlock, 0, stream>>>(a, l);
+            e = cudaGetLastError();
+            bound = std::min<long long>(bound * 8, 1ll << 32);
         }
-        workCount = hostCounters[2];
-        std::swap(workA, workB);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host, counters, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host + 4, a.counts, sizeof(int) * (kCollapseLevels + 1), cudaMemcpyDeviceToHost,
+                                stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess && (host[3] || host[4 + l] == 0)) break;   // error, or no level l
     }
     if (e != cudaSuccess)
     {
         err = std::string("BVH8 collapse: ") + cudaGetErrorString(e);
         return e == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA;
     }
-    nodeCount = hostCounters[0];
-    triCount = hostCounters[1];
+    if (host[3])
+    {
+        err = "BVH8 collapse exceeded its node or triangle capacity";
+        return PRT_EINTERNAL;
+    }
+    levels = 0;
+    while (levels <= kCollapseLevels && host[4 + levels] > 0) ++levels;
+    nodeCount = host[0];
+    triCount = host[1];
     return PRT_OK;
 }
 
@@ -688,7 +859,7 @@ struct Carve
 };
 
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
-               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping)
+               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping, DeviceScratch* scratch)
 {
     (void)nv;
     int status = PRT_OK;
@@ -701,12 +872,14 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     const int boundBlocks = std::min(1024, div_up(n, 256));
     const int nodeCapacity = std::max(1, nInternal);
     const bool group = PRT_WIDE_DP && sahGrouping && nInternal > 0;
+    int device = 0, numSMs = 148;
+    if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device);
 
     char* block = nullptr;
     float *triBox, *partial, *cbounds, *box;
     uint32_t *keysA, *keysB, *valsA, *valsB, *hist;
     int2 *child, *range, *workA, *workB;
-    int *parent, *flag, *counters;
+    int *parent, *flag, *counters, *counts;
     float4* dpCost;
     uint2* dpDec;
     auto carve = [&](char* base) {
@@ -727,6 +900,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         workA = c.take<int2>(nodeCapacity);
         workB = c.take<int2>(nodeCapacity);
         counters = c.take<int>(4);
+        counts = c.take<int>(kCollapseLevels + 1);
         dpCost = group ? c.take<float4>(2 * (size_t)nodeCapacity) : nullptr;
         dpDec = group ? c.take<uint2>(nodeCapacity) : nullptr;
         return c.off;
@@ -739,7 +913,15 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     BUILD_CHECK(cudaEventCreate(&ev1));
     BUILD_CHECK(cudaEventRecord(ev0, stream));
 
-    BUILD_CHECK(dev_malloc(&block, scratchBytes));
+    if (scratch)
+    {
+        BUILD_CHECK(scratch->reserve(scratchBytes));
+        block = static_cast<char*>(scratch->p);
+    }
+    else
+    {
+        BUILD_CHECK(dev_malloc(&block, scratchBytes));
+    }
     carve(block);
     {
         const size_t nodeBytes = (sizeof(Bvh8Node) * (size_t)nodeCapacity + 255) & ~(size_t)255;
@@ -799,30 +981,33 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         a.nodeCapacity = nodeCapacity;
         a.error = counters + 3;
         a.leafMax = std::max(1, std::min(3, leafMax));
-        a.dec = reinterpret_cast<const uint8_t*>(dpDec);
+        a.dec = dpDec;
+        a.counts = counts;
+        a.work[0] = workA;
+        a.work[1] = workB;
         int nodeCount = 0, triCount = 0;
-        status = collapse_levels(a, workA, workB, counters, n, stream, nodeCount, triCount, levels, err);
+        status = collapse_levels(a, counters, n, numSMs, stream, nodeCount, triCount, levels, err);
         if (status == PRT_OK && a.dec && 2 * levels > kStackMax)
         {
             // the SAH grouping came out deeper than the traversal stack allows
             // (possible for degenerate inputs): group greedily instead
             a.dec = nullptr;
-            status = collapse_levels(a, workA, workB, counters, n, stream, nodeCount, triCount, levels, err);
+            status = collapse_levels(a, counters, n, numSMs, stream, nodeCount, triCount, levels, err);
         }
         if (status != PRT_OK) goto done;
         out.nodeCount = nodeCount;
         out.triCount = triCount;
         out.leafMax = a.leafMax;
         out.levels = levels;
-        if (out.triCount != n)
-        {
-            err = "BVH8 collapse lost triangles";
-            status = PRT_EINTERNAL;
-            goto done;
-        }
         if (2 * levels > kStackMax)
         {
             err = "BVH8 is deeper than the traversal stack";
+            status = PRT_EINTERNAL;
+            goto done;
+        }
+        if (out.triCount != n)
+        {
+            err = "BVH8 collapse lost triangles";
             status = PRT_EINTERNAL;
             goto done;
         }
@@ -839,7 +1024,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     }
 
 done:
-    cudaFree(block);
+    if (!scratch) cudaFree(block);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (status != PRT_OK) out.release();

@@ -61,6 +61,7 @@ struct prt_ctx
 
     // acceleration structure
     Bvh8Device bvh;
+    DeviceScratch buildScratch;   // BVH build scratch, reused by rebuilds
     bool built = false;
     int leafMax = kDefaultLeafMax;
     bool highQuality = true;   // SAH grouping into 8-wide nodes
@@ -653,6 +654,7 @@ prt_ctx::~prt_ctx()
     cudaSetDevice(device);
     clear_graphs(this);
     bvh.release();
+    buildScratch.release();
     cudaFree(dPos);
     cudaFree(dIdx);
     cudaFree(dAlbedo);
@@ -845,7 +847,7 @@ int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats)
     BuildInfo info;
     std::string err;
     int st = build_bvh8(ctx->dPos, ctx->nv, ctx->dIdx, ctx->nt, ctx->bvh, ctx->stream, err, &info, ctx->leafMax,
-                        ctx->highQuality);
+                        ctx->highQuality, &ctx->buildScratch);
     if (st != PRT_OK) return fail(ctx, st, err);
     ctx->built = true;
     if (stats)

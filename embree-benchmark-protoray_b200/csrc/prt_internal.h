@@ -66,6 +66,32 @@ struct Bvh8Device
     }
 };
 
+// Device scratch kept between calls (a context's BVH builds): grows to the
+// largest request and is reused, so a rebuild allocates only its output.
+struct DeviceScratch
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+
+    cudaError_t reserve(size_t need)
+    {
+        if (need <= bytes) return cudaSuccess;
+        release();
+        char* q = nullptr;
+        cudaError_t e = dev_malloc(&q, need);
+        if (e != cudaSuccess) return e;
+        p = q;
+        bytes = need;
+        return cudaSuccess;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
 struct BuildInfo
 {
     double buildMs = 0;
@@ -73,8 +99,10 @@ struct BuildInfo
     int levels = 0;
 };
 
+// scratch: kept by the caller between builds, or nullptr for a temporary one
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
-               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping = true);
+               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping = true,
+               DeviceScratch* scratch = nullptr);
 
 // Sort and scan primitives (sort_scan.cu).  radix_sort_pairs sorts (key, value)
 // pairs stably on key bits [0, bits); the sorted pairs end in keys/vals (the

@@ -7,7 +7,7 @@
 // Steps (all on the device):
 //   1. triangle boxes + centroid bounds (block partials, one final reduce)
 //   2. 30-bit Morton codes of the centroids (10 bits per axis)
-//   3. stable LSD radix sort of (code, triangle) pairs, 4-bit digits
+//   3. stable LSD radix sort of (code, triangle) pairs, 8-bit digits
 //   4. binary radix tree over the sorted codes (Karras, HPG 2012); equal
 //      codes are ordered by their position, so duplicates are handled
 //   5. bottom-up bounds refit (second child to arrive computes the union),

@@ -108,7 +108,8 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
 // pairs stably on key bits [0, bits); the sorted pairs end in keys/vals (the
 // pointers are swapped with the temporaries as needed).  hist needs
 // radix_sort_hist_entries(n) words.  exclusive_scan_u32 writes the exclusive
-// prefix sums of in[0, n) to out and the total to sums[scan_sums_entries(n) - 1].
+// prefix sums of in[0, n) to out (in == out allowed) and the total to
+// sums[scan_sums_entries(n) - 1].
 // Both return the number of launches.
 size_t radix_sort_hist_entries(int n);
 int radix_sort_pairs(uint32_t*& keys, uint32_t*& vals, uint32_t*& keysTmp, uint32_t*& valsTmp, uint32_t* hist, int n,

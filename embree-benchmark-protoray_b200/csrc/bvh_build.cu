@@ -256,91 +256,130 @@ __device__ __forceinline__ void child_costs(const RefitArgs& a, int ref, const f
     c[4] = hi.x; c[5] = hi.y; c[6] = hi.z; c[7] = hi.w;
 }
 
+// Node `node` (children ch, triangle range rg) from its two finished
+// children: box, and with kGroup its grouping costs and decisions.
 template <bool kGroup>
-__global__ void k_refit(RefitArgs a)
+__device__ __forceinline__ void refit_node(const RefitArgs& a, int node, int2 ch, int2 rg)
 {
     const int n = a.n;
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    // leaf box
-    uint32_t p = a.vals[k];
-    float* lb = a.box + 6 * (size_t)((n - 1) + k);
+    const int ia = ch.x >= 0 ? ch.x : (n - 1) + ~ch.x;
+    const int ib = ch.y >= 0 ? ch.y : (n - 1) + ~ch.y;
+    float ba[6], bb[6], r[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) lb[c] = a.triBox[6 * (size_t)p + c];
-    int node = a.parent[(n - 1) + k];
-    while (node >= 0)
+    for (int c = 0; c < 6; ++c)
     {
-        __threadfence();
-        if (atomicAdd(&a.flag[node], 1) == 0) return;   // the sibling finishes this node
-        const int2 ch = a.child[node];
-        const int ia = ch.x >= 0 ? ch.x : (n - 1) + ~ch.x;
-        const int ib = ch.y >= 0 ? ch.y : (n - 1) + ~ch.y;
-        float ba[6], bb[6], r[6];
+        ba[c] = __ldcg(a.box + 6 * (size_t)ia + c);
+        bb[c] = __ldcg(a.box + 6 * (size_t)ib + c);
+    }
 #pragma unroll
-        for (int c = 0; c < 6; ++c)
+    for (int c = 0; c < 3; ++c)
+    {
+        r[c] = fminf(ba[c], bb[c]);
+        r[3 + c] = fmaxf(ba[3 + c], bb[3 + c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) __stcg(a.box + 6 * (size_t)node + c, r[c]);
+    if (kGroup)
+    {
+        float ca[8], cb[8];
+        child_costs(a, ch.x, ba, ca);
+        child_costs(a, ch.y, bb, cb);
+        const float area = box_half_area(r);
+        const int cnt = rg.y - rg.x + 1;
+        float dist[8];
+        uint8_t split[8];
+        dist[0] = FLT_MAX;
+        split[0] = 0;
+#pragma unroll
+        for (int i = 2; i <= 8; ++i)
         {
-            ba[c] = __ldcg(a.box + 6 * (size_t)ia + c);
-            bb[c] = __ldcg(a.box + 6 * (size_t)ib + c);
-        }
+            float best = FLT_MAX;
+            int bj = 1;
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-        {
-            r[c] = fminf(ba[c], bb[c]);
-            r[3 + c] = fmaxf(ba[3 + c], bb[3 + c]);
-        }
-#pragma unroll
-        for (int c = 0; c < 6; ++c) __stcg(a.box + 6 * (size_t)node + c, r[c]);
-        if (kGroup)
-        {
-            float ca[8], cb[8];
-            child_costs(a, ch.x, ba, ca);
-            child_costs(a, ch.y, bb, cb);
-            const float area = box_half_area(r);
-            const int2 rg = a.range[node];
-            const int cnt = rg.y - rg.x + 1;
-            float dist[8];
-            uint8_t split[8];
-            dist[0] = FLT_MAX;
-            split[0] = 0;
-#pragma unroll
-            for (int i = 2; i <= 8; ++i)
+            for (int j = 1; j < i; ++j)
             {
-                float best = FLT_MAX;
-                int bj = 1;
-#pragma unroll
-                for (int j = 1; j < i; ++j)
+                const float v = ca[j - 1] + cb[i - j - 1];
+                if (v < best)
                 {
-                    const float v = ca[j - 1] + cb[i - j - 1];
-                    if (v < best)
-                    {
-                        best = v;
-                        bj = j;
-                    }
+                    best = v;
+                    bj = j;
                 }
-                dist[i - 1] = best;
-                split[i - 1] = (uint8_t)bj;
             }
-            const float leafOpt = cnt <= a.leafMax ? area * PRT_SAH_CTRI * (float)cnt : FLT_MAX;
-            const float wideOpt = area + dist[7];
-            float cs[8];
-            float c = fminf(leafOpt, wideOpt);
-            cs[0] = c;
-            uint32_t d0 = leafOpt <= wideOpt ? 1u : 0u, d1 = 0;
-#pragma unroll
-            for (int i = 2; i <= 8; ++i)
-            {
-                uint32_t d = split[i - 1];
-                if (c <= dist[i - 1]) d |= 0x80;
-                else c = dist[i - 1];
-                cs[i - 1] = c;
-                if (i <= 4) d0 |= d << (8 * (i - 1));
-                else d1 |= d << (8 * (i - 5));
-            }
-            __stcg(a.cost + 2 * (size_t)node, make_float4(cs[0], cs[1], cs[2], cs[3]));
-            __stcg(a.cost + 2 * (size_t)node + 1, make_float4(cs[4], cs[5], cs[6], cs[7]));
-            __stcg(a.dec + node, make_uint2(d0, d1));
+            dist[i - 1] = best;
+            split[i - 1] = (uint8_t)bj;
         }
-        node = a.parent[node];
+        const float leafOpt = cnt <= a.leafMax ? area * PRT_SAH_CTRI * (float)cnt : FLT_MAX;
+        const float wideOpt = area + dist[7];
+        float cs[8];
+        float c = fminf(leafOpt, wideOpt);
+        cs[0] = c;
+        uint32_t d0 = leafOpt <= wideOpt ? 1u : 0u, d1 = 0;
+#pragma unroll
+        for (int i = 2; i <= 8; ++i)
+        {
+            uint32_t d = split[i - 1];
+            if (c <= dist[i - 1]) d |= 0x80;
+            else c = dist[i - 1];
+            cs[i - 1] = c;
+            if (i <= 4) d0 |= d << (8 * (i - 1));
+            else d1 |= d << (8 * (i - 5));
+        }
+        __stcg(a.cost + 2 * (size_t)node, make_float4(cs[0], cs[1], cs[2], cs[3]));
+        __stcg(a.cost + 2 * (size_t)node + 1, make_float4(cs[4], cs[5], cs[6], cs[7]));
+        __stcg(a.dec + node, make_uint2(d0, d1));
+    }
+}
+
+// The bottom-up walk with lanes refilled: each warp owns a run of consecutive
+// leaves; a lane whose walk ends (first arrival at a node, or the root) takes
+// the warp's next leaf, so the warp's lanes stay busy while the walks that
+// continue towards the root are short or long.
+constexpr int kRefitBlock = 256;
+
+template <bool kGroup>
+__global__ void __launch_bounds__(kRefitBlock) k_refit(RefitArgs a, int leavesPerWarp)
+{
+    const int n = a.n;
+    const int lane = threadIdx.x & 31;
+    const long long warpId = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    long long next = warpId * leavesPerWarp;
+    const long long end = min((long long)n, next + leavesPerWarp);
+    int node = -1;   // the node this lane arrives at next; -1: none
+    for (;;)
+    {
+        const unsigned idleMask = __ballot_sync(0xffffffffu, node < 0);
+        if (node < 0)
+        {
+            const long long k = next + __popc(idleMask & ((1u << lane) - 1u));
+            if (k < end)
+            {
+                // leaf box
+                const uint32_t p = a.vals[k];
+                float* lb = a.box + 6 * (size_t)((n - 1) + k);
+#pragma unroll
+                for (int c = 0; c < 6; ++c) lb[c] = a.triBox[6 * (size_t)p + c];
+                node = a.parent[(n - 1) + k];
+            }
+        }
+        next += __popc(idleMask);
+        if (!__any_sync(0xffffffffu, node >= 0) && next >= end) break;
+        if (node >= 0)
+        {
+            // the tree links are read-only here: fetch them before the arrival
+            const int2 ch = a.child[node];
+            const int2 rg = kGroup ? a.range[node] : make_int2(0, 0);
+            const int up = a.parent[node];
+            __threadfence();
+            if (atomicAdd(&a.flag[node], 1) == 0)
+            {
+                node = -1;   // the sibling finishes this node
+            }
+            else
+            {
+                refit_node<kGroup>(a, node, ch, rg);
+                node = up;
+            }
+        }
     }
 }
 
@@ -842,22 +881,6 @@ int collapse_levels(const CollapseArgs& a, int* counters, int n, int numSMs, cud
         }                                                                                                      \
     } while (0)
 
-// Scratch buffers of one build, carved from one allocation (each 256-byte
-// aligned): a dry run with a null base measures the block.
-struct Carve
-{
-    char* base;
-    size_t off = 0;
-    template <class T>
-    T* take(size_t count)
-    {
-        off = (off + 255) & ~(size_t)255;
-        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
-        off += sizeof(T) * count;
-        return p;
-    }
-};
-
 int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
                std::string& err, BuildInfo* info, int leafMax, bool sahGrouping, DeviceScratch* scratch)
 {
@@ -960,8 +983,13 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         ra.cost = dpCost;
         ra.dec = dpDec;
         ra.leafMax = std::max(1, std::min(3, leafMax));
-        if (group) k_refit<true><<<div_up(n, 256), 256, 0, stream>>>(ra);
-        else k_refit<false><<<div_up(n, 256), 256, 0, stream>>>(ra);
+        int perSM = 1;
+        if (group) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_refit<true>, kRefitBlock, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_refit<false>, kRefitBlock, 0);
+        const int blocks = std::max(1, std::min(std::max(1, perSM) * numSMs, div_up(n, kRefitBlock)));
+        const int leavesPerWarp = div_up(n, (long long)blocks * (kRefitBlock / 32));
+        if (group) k_refit<true><<<blocks, kRefitBlock, 0, stream>>>(ra, leavesPerWarp);
+        else k_refit<false><<<blocks, kRefitBlock, 0, stream>>>(ra, leavesPerWarp);
     }
     BUILD_CHECK(cudaGetLastError());
 

@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(256) k_soup_expand(const float* __restrict__ v
 } // namespace
 
 int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream, BuiltMesh& out, std::string& err,
-                   double* buildMs, long long* launchesOut, bool soupOnDevice)
+                   double* buildMs, long long* launchesOut, bool soupOnDevice, DeviceScratch* scratch)
 {
     out.release();
     if (n < 0 || n > 0x7fffffff / 3)
@@ -385,6 +385,7 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
     uint32_t tableSize = 1024;
     while (tableSize < 2u * (uint32_t)std::max(nc, 1)) tableSize <<= 1;
 
+    char* block = nullptr;        // the scratch buffers below
     float* soup = nullptr;
     float* partial = nullptr;
     float* bounds = nullptr;      // [6]
@@ -413,26 +414,47 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
 
     MB_CHECK(cudaEventCreate(&ev0));
     MB_CHECK(cudaEventCreate(&ev1));
-    MB_CHECK(dev_malloc(&small, sizeof(unsigned) * 2));
-    MB_CHECK(dev_malloc(&bounds, sizeof(float) * 6));
-    MB_CHECK(dev_malloc(&partial, sizeof(float) * 6 * (size_t)scanBlocks));
+    {
+        // every scratch buffer in one block
+        const size_t hc = n > 0 ? radix_sort_hist_entries(std::max(n, nc)) : 0;
+        auto carve = [&](char* base) {
+            Carve c{base};
+            small = c.take<unsigned>(2);
+            bounds = c.take<float>(6);
+            partial = c.take<float>(6 * (size_t)scanBlocks);
+            if (n > 0)
+            {
+                if (!soupOnDevice) soup = c.take<float>(sizeof(prt_soup_triangle) / sizeof(float) * (size_t)n);
+                corners = c.take<float4>(2 * (size_t)nc);
+                triKeys = c.take<uint32_t>(n);
+                triVals = c.take<uint32_t>(n);
+                keysTmp = c.take<uint32_t>(nc);
+                valsTmp = c.take<uint32_t>(nc);
+                hist = c.take<uint32_t>(hc);
+                table = c.take<uint32_t>(tableSize);
+                slotOf = c.take<int>(nc);
+                rep = c.take<int>(nc);
+                unique = c.take<uint32_t>(nc);
+                pos = c.take<uint32_t>(nc);
+                sums = c.take<uint32_t>(scan_sums_entries(nc));
+            }
+            return c.off;
+        };
+        const size_t bytes = carve(nullptr);
+        if (scratch)
+        {
+            MB_CHECK(scratch->reserve(bytes));
+            block = static_cast<char*>(scratch->p);
+        }
+        else
+        {
+            MB_CHECK(dev_malloc(&block, bytes));
+        }
+        carve(block);
+    }
     if (n > 0)
     {
-        const size_t hc = radix_sort_hist_entries(std::max(n, nc));
         if (soupOnDevice) soup = const_cast<float*>(reinterpret_cast<const float*>(hostTris));
-        else MB_CHECK(dev_malloc(&soup, sizeof(prt_soup_triangle) * (size_t)n));
-        MB_CHECK(dev_malloc(&corners, sizeof(float4) * 2 * (size_t)nc));
-        MB_CHECK(dev_malloc(&triKeys, sizeof(uint32_t) * (size_t)n));
-        MB_CHECK(dev_malloc(&triVals, sizeof(uint32_t) * (size_t)n));
-        MB_CHECK(dev_malloc(&keysTmp, sizeof(uint32_t) * (size_t)nc));
-        MB_CHECK(dev_malloc(&valsTmp, sizeof(uint32_t) * (size_t)nc));
-        MB_CHECK(dev_malloc(&hist, sizeof(uint32_t) * hc));
-        MB_CHECK(dev_malloc(&table, sizeof(uint32_t) * (size_t)tableSize));
-        MB_CHECK(dev_malloc(&slotOf, sizeof(int) * (size_t)nc));
-        MB_CHECK(dev_malloc(&rep, sizeof(int) * (size_t)nc));
-        MB_CHECK(dev_malloc(&unique, sizeof(uint32_t) * (size_t)nc));
-        MB_CHECK(dev_malloc(&pos, sizeof(uint32_t) * (size_t)nc));
-        MB_CHECK(dev_malloc(&sums, sizeof(uint32_t) * scan_sums_entries(nc)));
         if (!soupOnDevice)
             MB_CHECK(cudaMemcpyAsync(soup, hostTris, sizeof(prt_soup_triangle) * (size_t)n, cudaMemcpyDefault, stream));
     }
@@ -470,9 +492,20 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
     out.stride = 3 + (out.hasNormals ? 3 : 0) + (out.hasTexcoords ? 2 : 0);
     std::memcpy(out.lo, hb, 12);
     std::memcpy(out.hi, hb + 3, 12);
-    MB_CHECK(dev_malloc(&out.idx, sizeof(int) * 3 * (size_t)std::max(n, 1)));
-    MB_CHECK(dev_malloc(&out.mat, sizeof(int) * (size_t)std::max(n, 1)));
-    MB_CHECK(dev_malloc(&out.attr, sizeof(float) * out.stride * (size_t)std::max(out.vertCount, 1)));
+    {
+        // the outputs in one block
+        auto carveOut = [&](char* base) {
+            Carve c{base};
+            out.idx = c.take<int>(3 * (size_t)std::max(n, 1));
+            out.mat = c.take<int>((size_t)std::max(n, 1));
+            out.attr = c.take<float>((size_t)out.stride * (size_t)std::max(out.vertCount, 1));
+            return c.off;
+        };
+        char* ob = nullptr;
+        MB_CHECK(dev_malloc(&ob, carveOut(nullptr)));
+        out.block = ob;
+        carveOut(ob);
+    }
     if (n > 0)
     {
         const int nv = out.vertCount;
@@ -510,22 +543,7 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
 
 done:
 #undef MB_CHECK
-    if (!soupOnDevice) cudaFree(soup);
-    cudaFree(partial);
-    cudaFree(bounds);
-    cudaFree(small);
-    cudaFree(corners);
-    cudaFree(triKeys);
-    cudaFree(triVals);
-    cudaFree(keysTmp);
-    cudaFree(valsTmp);
-    cudaFree(hist);
-    cudaFree(table);
-    cudaFree(slotOf);
-    cudaFree(rep);
-    cudaFree(unique);
-    cudaFree(pos);
-    cudaFree(sums);
+    if (!scratch) cudaFree(block);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (status != PRT_OK) out.release();
@@ -534,7 +552,7 @@ done:
 }
 
 int build_mesh_gpu_indexed(const SoupIndexed& s, cudaStream_t stream, BuiltMesh& out, std::string& err, double* buildMs,
-                           long long* launchesOut)
+                           long long* launchesOut, DeviceScratch* scratch)
 {
     out.release();
     if (s.triCount < 0 || s.triCount > 0x7fffffff / 3)
@@ -543,23 +561,31 @@ int build_mesh_gpu_indexed(const SoupIndexed& s, cudaStream_t stream, BuiltMesh&
         return PRT_EINVAL;
     }
     const int n = (int)s.triCount;
-    if (n == 0) return build_mesh_gpu(nullptr, 0, stream, out, err, buildMs, launchesOut, false);
+    if (n == 0) return build_mesh_gpu(nullptr, 0, stream, out, err, buildMs, launchesOut, false, scratch);
     int status = PRT_OK;
     float *dv = nullptr, *dvt = nullptr, *dvn = nullptr, *dsoup = nullptr;
     int *dcorners = nullptr, *dmat = nullptr;
-    const size_t cornerBytes = sizeof(int) * 3 * (size_t)s.cornerInts * (size_t)n;
-    cudaError_t e = dev_malloc(&dv, sizeof(float) * 3 * (size_t)std::max(1LL, s.nv));
-    if (e == cudaSuccess && s.nvt) e = dev_malloc(&dvt, sizeof(float) * 2 * (size_t)s.nvt);
-    if (e == cudaSuccess && s.nvn) e = dev_malloc(&dvn, sizeof(float) * 3 * (size_t)s.nvn);
-    if (e == cudaSuccess) e = dev_malloc(&dcorners, cornerBytes);
-    if (e == cudaSuccess) e = dev_malloc(&dmat, sizeof(int) * (size_t)n);
-    if (e == cudaSuccess) e = dev_malloc(&dsoup, sizeof(prt_soup_triangle) * (size_t)n);
+    const size_t cornerInts = 3 * (size_t)s.cornerInts * (size_t)n;
+    // the uploaded lists and the expanded records in one block
+    auto carve = [&](char* base) {
+        Carve c{base};
+        dv = c.take<float>(3 * (size_t)std::max(1LL, s.nv));
+        dvt = s.nvt ? c.take<float>(2 * (size_t)s.nvt) : nullptr;
+        dvn = s.nvn ? c.take<float>(3 * (size_t)s.nvn) : nullptr;
+        dcorners = c.take<int>(cornerInts);
+        dmat = c.take<int>((size_t)n);
+        dsoup = c.take<float>(sizeof(prt_soup_triangle) / sizeof(float) * (size_t)n);
+        return c.off;
+    };
+    char* block = nullptr;
+    cudaError_t e = dev_malloc(&block, carve(nullptr));
+    if (e == cudaSuccess) carve(block);
     if (e == cudaSuccess && s.nv) e = cudaMemcpyAsync(dv, s.v, sizeof(float) * 3 * (size_t)s.nv, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess && s.nvt)
         e = cudaMemcpyAsync(dvt, s.vt, sizeof(float) * 2 * (size_t)s.nvt, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess && s.nvn)
         e = cudaMemcpyAsync(dvn, s.vn, sizeof(float) * 3 * (size_t)s.nvn, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dcorners, s.corners, cornerBytes, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dcorners, s.corners, sizeof(int) * cornerInts, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dmat, s.mat, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess)
     {
@@ -575,14 +601,9 @@ int build_mesh_gpu_indexed(const SoupIndexed& s, cudaStream_t stream, BuiltMesh&
     else
     {
         status = build_mesh_gpu(reinterpret_cast<const prt_soup_triangle*>(dsoup), n, stream, out, err, buildMs,
-                                launchesOut, true);
+                                launchesOut, true, scratch);
     }
-    cudaFree(dv);
-    cudaFree(dvt);
-    cudaFree(dvn);
-    cudaFree(dcorners);
-    cudaFree(dmat);
-    cudaFree(dsoup);
+    cudaFree(block);
     return status;
 }
 

@@ -61,7 +61,7 @@ struct prt_ctx
 
     // acceleration structure
     Bvh8Device bvh;
-    DeviceScratch buildScratch;   // BVH build scratch, reused by rebuilds
+    DeviceScratch buildScratch;   // BVH and mesh build scratch, reused by later builds
     bool built = false;
     int leafMax = kDefaultLeafMax;
     bool highQuality = true;   // SAH grouping into 8-wide nodes
@@ -1466,7 +1466,8 @@ int prt_build_mesh(prt_ctx* ctx, const prt_soup_triangle* tris, int triCount, co
     CK(cudaSetDevice(ctx->device));
     const auto t0 = std::chrono::steady_clock::now();
     double buildMs = 0;
-    int st = build_mesh_gpu(tris, triCount, ctx->stream, ctx->builtMesh, ctx->err, &buildMs, &ctx->launches);
+    int st = build_mesh_gpu(tris, triCount, ctx->stream, ctx->builtMesh, ctx->err, &buildMs, &ctx->launches, false,
+                            &ctx->buildScratch);
     if (st != PRT_OK) return st;
     const auto t1 = std::chrono::steady_clock::now();
     BuiltMesh& m = ctx->builtMesh;
@@ -1494,7 +1495,8 @@ int prt_build_mesh_soup(prt_ctx* ctx, const prt_soup* soup, prt_mesh_info* info)
     CK(cudaSetDevice(ctx->device));
     const auto t0 = std::chrono::steady_clock::now();
     double buildMs = 0;
-    int st = build_mesh_gpu_indexed(s, ctx->stream, ctx->builtMesh, ctx->err, &buildMs, &ctx->launches);
+    int st = build_mesh_gpu_indexed(s, ctx->stream, ctx->builtMesh, ctx->err, &buildMs, &ctx->launches,
+                                    &ctx->buildScratch);
     if (st != PRT_OK) return st;
     const auto t1 = std::chrono::steady_clock::now();
     BuiltMesh& m = ctx->builtMesh;

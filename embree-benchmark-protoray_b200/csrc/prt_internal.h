@@ -66,8 +66,24 @@ struct Bvh8Device
     }
 };
 
-// Device scratch kept between calls (a context's BVH builds): grows to the
-// largest request and is reused, so a rebuild allocates only its output.
+// Buffers carved from one allocation, each 256-byte aligned: a dry run with a
+// null base measures the block, a second run with the block hands them out.
+struct Carve
+{
+    char* base;
+    size_t off = 0;
+    template <class T>
+    T* take(size_t count)
+    {
+        off = (off + 255) & ~(size_t)255;
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += sizeof(T) * count;
+        return p;
+    }
+};
+
+// Device scratch kept between calls (a context's BVH and mesh builds): grows
+// to the largest request and is reused, so a rebuild allocates only its output.
 struct DeviceScratch
 {
     void* p = nullptr;
@@ -120,6 +136,7 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t* sums, int n,
 // An indexed mesh built from a triangle soup on the device (mesh_build.cu).
 struct BuiltMesh
 {
+    void* block = nullptr;  // the allocation holding idx, mat and attr
     int* idx = nullptr;     // [3 * triCount]
     int* mat = nullptr;     // [triCount]
     float* attr = nullptr;  // [vertCount * stride]: position [, normal] [, texcoord], as in the .mesh blob
@@ -131,9 +148,8 @@ struct BuiltMesh
 
     void release()
     {
-        cudaFree(idx);
-        cudaFree(mat);
-        cudaFree(attr);
+        if (block) cudaFree(block);
+        block = nullptr;
         idx = mat = nullptr;
         attr = nullptr;
         triCount = vertCount = 0;
@@ -145,12 +161,13 @@ struct BuiltMesh
 // TriangleMeshBuilder on the device; hostTris may be host or device memory
 // (soupOnDevice: device memory the builder may read in place).  On success
 // `out` owns the mesh (names are left to the caller).
+// scratch: kept by the caller between builds, or nullptr for a temporary one.
 int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream, BuiltMesh& out, std::string& err,
-                   double* buildMs, long long* launches, bool soupOnDevice = false);
+                   double* buildMs, long long* launches, bool soupOnDevice = false, DeviceScratch* scratch = nullptr);
 // The same for a parsed OBJ soup: uploads its indexed form and expands the
 // triangle records on the device.
 int build_mesh_gpu_indexed(const SoupIndexed& soup, cudaStream_t stream, BuiltMesh& out, std::string& err,
-                           double* buildMs, long long* launches);
+                           double* buildMs, long long* launches, DeviceScratch* scratch = nullptr);
 
 // Arguments of one wave of the wavefront renderer.
 struct WaveArgs

@@ -228,12 +228,14 @@ def test_builder_errors(ctx, tmp_path):
     c.close()
 
 
-def test_builder_allocation_failures(obj_golden, ctx):
+def test_builder_allocation_failures(obj_golden):
     """Every device allocation of the builder failing in turn gives PRT_ENOMEM
-    and leaves the context usable."""
+    and leaves the context usable.  A fresh context allocates the build scratch
+    (kept for later builds) and then the output, so two failures are seen."""
     import prt
     j = list(obj_golden["mesh_names"]).index("random_normals")
     t, n = obj_golden[f"mesh_soup_{j}"], _names(obj_golden[f"mesh_mtl_{j}"])
+    ctx = prt.Context(0)
     seen = 0
     for k in range(40):
         prt.fail_allocations(k)
@@ -245,8 +247,9 @@ def test_builder_allocation_failures(obj_golden, ctx):
             seen += 1
         finally:
             prt.fail_allocations(-1)
-    assert seen >= 10
+    assert seen >= 2
     ctx.build_mesh(t, n)
+    ctx.close()
 
 
 def test_cli_build(obj_golden, tmp_path):

@@ -396,14 +396,13 @@ struct CollapseArgs
     const int* idx;
     Bvh8Node* nodes;
     TriRec* tris;
-    int* nodeCounter;
-    int* triCounter;
+    unsigned long long* alloc;   // 8-wide nodes allocated (high 32 bits), leaf triangles (low 32 bits)
     int nodeCapacity;
     int* error;
     int leafMax;          // subtrees of at most this many triangles (1..3) become leaves
     const uint2* dec;     // grouping decisions of k_refit<true>, or nullptr for the greedy grouping
-    int* counts;          // work items per level: counts[l] items of level l, kCollapseLevels + 1 entries
-    int2* work[2];        // work items of even / odd levels
+    int* binRef;          // per 8-wide node: the binary reference it is built from
+    int* marks;           // level l is nodes [marks[l], marks[l + 1]); kCollapseLevels + 2 entries
 };
 
 // Levels launched; a tree that needs more would overflow the traversal stack
@@ -444,14 +443,12 @@ struct __align__(16) CollapseGroup
     int2 front[8];
 };
 
-// One 8-lane group builds one 8-wide node: lane c holds child c of the node.
-// Work item: (binary reference, 8-wide node index).  A binary reference of
+// One 8-lane group builds 8-wide node nodeIdx from binary reference
+// binRef[nodeIdx]: lane c holds child c of the node.  A binary reference of
 // ~0 with n == 1 is the single-triangle scene.
-__device__ void collapse_node(const CollapseArgs& a, int2 item, int level, int sub, unsigned gmask,
-                              CollapseGroup& g)
+__device__ void collapse_node(const CollapseArgs& a, int nodeIdx, int sub, unsigned gmask, CollapseGroup& g)
 {
-    const int bref = item.x;
-    const int nodeIdx = item.y;
+    const int bref = a.binRef[nodeIdx];
 
     // 1. children: the roots chosen by the grouping decisions (or greedily
     //    opened), left to right in tree order, child c in lane c
@@ -681,20 +678,35 @@ __device__ void collapse_node(const CollapseArgs& a, int2 item, int level, int s
             nTris += c;
         }
     }
-    int childBase = 0, triBase = 0, nextBase = 0, bad = 0;
+    int childBase = 0, triBase = 0, bad = 0;
     if (sub == 0)
     {
-        childBase = nInternal ? atomicAdd(a.nodeCounter, nInternal) : 0;
-        triBase = nTris ? atomicAdd(a.triCounter, nTris) : 0;
+        // one atomic for the child nodes and leaf triangles of all the groups
+        // of this warp that are here together
+        const unsigned m = __activemask();
+        const int me = threadIdx.x & 31;
+        const unsigned long long req = ((unsigned long long)nInternal << 32) | (unsigned)nTris;
+        unsigned long long before = 0, total = 0;
+        for (unsigned rest = m; rest; rest &= rest - 1)
+        {
+            const int l = __ffs(rest) - 1;
+            const unsigned long long v = __shfl_sync(m, req, l);
+            if (l < me) before += v;
+            total += v;
+        }
+        const int first = __ffs(m) - 1;
+        unsigned long long base = 0;
+        if (me == first) base = atomicAdd(a.alloc, total);
+        base = __shfl_sync(m, base, first) + before;
+        childBase = (int)(base >> 32);
+        triBase = (int)(base & 0xffffffffu);
         bad = childBase + nInternal > a.nodeCapacity || triBase + nTris > a.n;
         if (bad) atomicExch(a.error, 1);
-        else if (nInternal) nextBase = atomicAdd(a.counts + level + 1, nInternal);
     }
     const int leader = __ffs(gmask) - 1;
     if (__shfl_sync(gmask, bad, leader)) return;   // group-uniform
     childBase = __shfl_sync(gmask, childBase, leader);
     triBase = __shfl_sync(gmask, triBase, leader);
-    nextBase = __shfl_sync(gmask, nextBase, leader);
 
     // 6. header: per-axis power-of-two scale s with the node box spanning at
     //    most 253 steps, and origin one step below the box, so every quantized
@@ -760,7 +772,7 @@ __device__ void collapse_node(const CollapseArgs& a, int2 item, int level, int s
         if (!leaf)
         {
             g.node[24 + slot] = (uint8_t)(0x20 | (24 + slot));
-            a.work[(level + 1) & 1][nextBase + internalRank] = make_int2(r, childBase + internalRank);
+            a.binRef[childBase + internalRank] = r;
         }
         else
         {
@@ -794,76 +806,89 @@ __device__ void collapse_node(const CollapseArgs& a, int2 item, int level, int s
     __syncwarp(gmask);
 }
 
-// One tree level: the items of counts[level], one per 8-lane group, grid-strided.
+// One tree level: nodes [marks[level], marks[level + 1]), one per 8-lane
+// group, grid-strided.
 __global__ void __launch_bounds__(kCollapseBlock) k_collapse(CollapseArgs a, int level)
 {
     __shared__ CollapseGroup groups[kGroupsPerBlock];
     if (*(volatile int*)a.error) return;
-    const int count = *(volatile int*)(a.counts + level);
+    const int begin = *(volatile int*)(a.marks + level);
+    const int end = *(volatile int*)(a.marks + level + 1);
     const int lane = threadIdx.x & 31;
     const int sub = lane & 7;
     const unsigned gmask = 0xffu << (lane & 24);
     CollapseGroup& g = groups[threadIdx.x >> 3];
-    const int2* work = a.work[level & 1];
     const int stride = gridDim.x * kGroupsPerBlock;
-    for (int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 3); w < count; w += stride)
-        collapse_node(a, work[w], level, sub, gmask, g);
+    for (int w = begin + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 3); w < end; w += stride)
+        collapse_node(a, w, sub, gmask, g);
+}
+
+// After level l: the nodes allocated so far end level l + 1.
+__global__ void k_collapse_mark(CollapseArgs a, int level)
+{
+    a.marks[level + 2] = (int)(*(volatile unsigned long long*)a.alloc >> 32);
 }
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 // Runs the collapse from the root, one launch per level, without waiting for
-// the host between levels: launches past the last level find no items and
+// the host between levels: launches past the last level find no nodes and
 // return.  The counters are read back after the first kCollapseBatch levels
 // and, for a deeper tree, after the rest.  On success sets the node and
 // triangle counts and the number of 8-wide levels (kCollapseLevels + 1 for a
 // tree deeper than the launches).
 constexpr int kCollapseBatch = 16;
 
-int collapse_levels(const CollapseArgs& a, int* counters, int n, int numSMs, cudaStream_t stream,
-                    int& nodeCount, int& triCount, int& levels, std::string& err)
+int collapse_levels(const CollapseArgs& a, int n, int numSMs, cudaStream_t stream, int& nodeCount, int& triCount,
+                    int& levels, std::string& err)
 {
-    int2 root = make_int2(n > 1 ? 0 : ~0, 0);
-    int init[4] = {1, 0, 0, 0};   // nodeCounter, triCounter, unused, error
-    int host[4 + kCollapseLevels + 1];
-    cudaError_t e = cudaMemcpyAsync(a.work[0], &root, sizeof(int2), cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(a.counts, 0, sizeof(int) * (kCollapseLevels + 1), stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(a.counts, &init[0], sizeof(int), cudaMemcpyHostToDevice, stream);
-    const long long maxBlocks = (long long)std::max(1, numSMs) * 8;
-    long long bound = 1;   // level l holds at most 8^l items
+    const int root = n > 1 ? 0 : ~0;
+    const unsigned long long alloc0 = 1ull << 32;   // the root
+    const int marks0[2] = {0, 1};
+    int hostErr = 0;
+    unsigned long long hostAlloc = 0;
+    int marks[kCollapseLevels + 2];
+    cudaError_t e = cudaMemcpyAsync(a.binRef, &root, sizeof(int), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a.alloc, &alloc0, sizeof(alloc0), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.error, 0, sizeof(int), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.marks, 0, sizeof(int) * (kCollapseLevels + 2), stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a.marks, marks0, sizeof(marks0), cudaMemcpyHostToDevice, stream);
+    int perSM = 1;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_collapse, kCollapseBlock, 0);
+    const long long maxBlocks = (long long)std::max(1, numSMs) * std::max(1, perSM);
+    long long bound = 1;   // level l holds at most 8^l nodes
     int l = 0;
     while (e == cudaSuccess && l < kCollapseLevels)
     {
-        const int end = std::min(kCollapseLevels, l + kCollapseBatch);
-        for (; e == cudaSuccess && l < end; ++l)
+        const int stop = std::min(kCollapseLevels, l + kCollapseBatch);
+        for (; e == cudaSuccess && l < stop; ++l)
         {
             const int blocks = (int)std::min(maxBlocks, (bound + kGroupsPerBlock - 1) / kGroupsPerBlock);
             k_collapse<<<blocks, kCollapseBlock, 0, stream>>>(a, l);
+            k_collapse_mark<<<1, 1, 0, stream>>>(a, l);
             e = cudaGetLastError();
             bound = std::min<long long>(bound * 8, 1ll << 32);
         }
-        if (e == cudaSuccess) e = cudaMemcpyAsync(host, counters, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(host + 4, a.counts, sizeof(int) * (kCollapseLevels + 1), cudaMemcpyDeviceToHost,
-                                stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hostErr, a.error, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hostAlloc, a.alloc, sizeof(hostAlloc), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(marks, a.marks, sizeof(marks), cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e == cudaSuccess && (host[3] || host[4 + l] == 0)) break;   // error, or no level l
+        if (e == cudaSuccess && (hostErr || marks[l + 1] == marks[l])) break;   // error, or no level l
     }
     if (e != cudaSuccess)
     {
         err = std::string("BVH8 collapse: ") + cudaGetErrorString(e);
         return e == cudaErrorMemoryAllocation ? PRT_ENOMEM : PRT_ECUDA;
     }
-    if (host[3])
+    if (hostErr)
     {
         err = "BVH8 collapse exceeded its node or triangle capacity";
         return PRT_EINTERNAL;
     }
     levels = 0;
-    while (levels <= kCollapseLevels && host[4 + levels] > 0) ++levels;
-    nodeCount = host[0];
-    triCount = host[1];
+    while (levels <= kCollapseLevels && marks[levels + 1] > marks[levels]) ++levels;
+    nodeCount = (int)(hostAlloc >> 32);
+    triCount = (int)(hostAlloc & 0xffffffffu);
     return PRT_OK;
 }
 
@@ -901,8 +926,9 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     char* block = nullptr;
     float *triBox, *partial, *cbounds, *box;
     uint32_t *keysA, *keysB, *valsA, *valsB, *hist;
-    int2 *child, *range, *workA, *workB;
-    int *parent, *flag, *counters, *counts;
+    int2 *child, *range;
+    int *parent, *flag, *collapseErr, *marks, *binRef;
+    unsigned long long* collapseAlloc;
     float4* dpCost;
     uint2* dpDec;
     auto carve = [&](char* base) {
@@ -920,10 +946,10 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         parent = c.take<int>(2 * (size_t)n);
         flag = c.take<int>(nodeCapacity);
         box = c.take<float>(6 * (size_t)(2 * n));
-        workA = c.take<int2>(nodeCapacity);
-        workB = c.take<int2>(nodeCapacity);
-        counters = c.take<int>(4);
-        counts = c.take<int>(kCollapseLevels + 1);
+        binRef = c.take<int>(nodeCapacity);
+        collapseAlloc = c.take<unsigned long long>(1);
+        collapseErr = c.take<int>(1);
+        marks = c.take<int>(kCollapseLevels + 2);
         dpCost = group ? c.take<float4>(2 * (size_t)nodeCapacity) : nullptr;
         dpDec = group ? c.take<uint2>(nodeCapacity) : nullptr;
         return c.off;
@@ -1004,23 +1030,21 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         a.idx = dIdx;
         a.nodes = out.nodes;
         a.tris = out.tris;
-        a.nodeCounter = counters + 0;
-        a.triCounter = counters + 1;
+        a.alloc = collapseAlloc;
         a.nodeCapacity = nodeCapacity;
-        a.error = counters + 3;
+        a.error = collapseErr;
         a.leafMax = std::max(1, std::min(3, leafMax));
         a.dec = dpDec;
-        a.counts = counts;
-        a.work[0] = workA;
-        a.work[1] = workB;
+        a.binRef = binRef;
+        a.marks = marks;
         int nodeCount = 0, triCount = 0;
-        status = collapse_levels(a, counters, n, numSMs, stream, nodeCount, triCount, levels, err);
+        status = collapse_levels(a, n, numSMs, stream, nodeCount, triCount, levels, err);
         if (status == PRT_OK && a.dec && 2 * levels > kStackMax)
         {
             // the SAH grouping came out deeper than the traversal stack allows
             // (possible for degenerate inputs): group greedily instead
             a.dec = nullptr;
-            status = collapse_levels(a, counters, n, numSMs, stream, nodeCount, triCount, levels, err);
+            status = collapse_levels(a, n, numSMs, stream, nodeCount, triCount, levels, err);
         }
         if (status != PRT_OK) goto done;
         out.nodeCount = nodeCount;

@@ -330,6 +330,15 @@ __device__ __forceinline__ void refit_node(const RefitArgs& a, int node, int2 ch
     }
 }
 
+// Arrival at a node: the atomic increment releases this thread's writes (its
+// child's box and costs) and, for the second arrival, acquires the sibling's.
+__device__ __forceinline__ unsigned arrive(int* flag)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(flag) : "memory");
+    return old;
+}
+
 // The bottom-up walk with lanes refilled: each warp owns a run of consecutive
 // leaves; a lane whose walk ends (first arrival at a node, or the root) takes
 // the warp's next leaf, so the warp's lanes stay busy while the walks that
@@ -369,8 +378,7 @@ __global__ void __launch_bounds__(kRefitBlock) k_refit(RefitArgs a, int leavesPe
             const int2 ch = a.child[node];
             const int2 rg = kGroup ? a.range[node] : make_int2(0, 0);
             const int up = a.parent[node];
-            __threadfence();
-            if (atomicAdd(&a.flag[node], 1) == 0)
+            if (arrive(a.flag + node) == 0)
             {
                 node = -1;   // the sibling finishes this node
             }

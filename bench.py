@@ -15,6 +15,7 @@ region is bracketed by barriers and the max over ranks is reported.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import math
 import os
@@ -157,7 +158,31 @@ def sum_over_ranks(x, dist, device):
     return float(t.item())
 
 
+@contextlib.contextmanager
+def c_stdout_to_stderr():
+    """The reference's host code logs its progress to stdout; while it runs,
+    file descriptor 1 points at stderr, so that this script's stdout carries
+    only the JSON line."""
+    import ctypes
+    libc = ctypes.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None):
+    with c_stdout_to_stderr():
+        return _cpu_reference_run(steps, warmup, frames_per_step, sample_seconds)
+
+
+def _cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None):
     """Times the reference's own diffuseStream renderer (oracle/_ref) on the
     host cores at 1920x1080, maxDepth 5; one step = `frames_per_step` frames."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -362,7 +387,7 @@ def run_mesh_build(prt, torch, device):
             np.savetxt(f, mesh.indices + 1, fmt="f %d %d %d")
         c = prt.Context(device)
         best = None
-        for _ in range(4):
+        for _ in range(6):
             t0 = time.perf_counter()
             soup = prt.Soup(obj)
             t1 = time.perf_counter()
@@ -386,11 +411,12 @@ def run_mesh_build(prt, torch, device):
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import oracle
             R = oracle.Reference()
-            t0 = time.perf_counter()
-            rt, rn = R.load_obj(obj)
-            t1 = time.perf_counter()
-            build_ms = R.build_soup(rt, rn, os.path.join(d, "terrain_ref.mesh"))
-            t2 = time.perf_counter()
+            with c_stdout_to_stderr():
+                t0 = time.perf_counter()
+                rt, rn = R.load_obj(obj)
+                t1 = time.perf_counter()
+                build_ms = R.build_soup(rt, rn, os.path.join(d, "terrain_ref.mesh"))
+                t2 = time.perf_counter()
             out["reference"] = {"parse_ms": round((t1 - t0) * 1e3, 1), "build_ms": round(build_ms, 1),
                                 "e2e_ms": round((t2 - t0) * 1e3, 1),
                                 "kind": "reference ObjLoader + TriangleMeshBuilder compiled from source, 1 thread"}

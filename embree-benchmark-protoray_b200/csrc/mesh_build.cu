@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(256) k_soup_expand(const float* __restrict__ v
 int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream, BuiltMesh& out, std::string& err,
                    double* buildMs, long long* launchesOut, bool soupOnDevice, DeviceScratch* scratch)
 {
-    out.release();
+    out.reset();
     if (n < 0 || n > 0x7fffffff / 3)
     {
         err = "triangle count out of range";
@@ -501,10 +501,18 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
             out.attr = c.take<float>((size_t)out.stride * (size_t)std::max(out.vertCount, 1));
             return c.off;
         };
-        char* ob = nullptr;
-        MB_CHECK(dev_malloc(&ob, carveOut(nullptr)));
-        out.block = ob;
-        carveOut(ob);
+        const size_t bytes = carveOut(nullptr);
+        if (out.blockBytes < bytes)
+        {
+            if (out.block) cudaFree(out.block);
+            out.block = nullptr;
+            out.blockBytes = 0;
+            char* ob = nullptr;
+            MB_CHECK(dev_malloc(&ob, bytes));
+            out.block = ob;
+            out.blockBytes = bytes;
+        }
+        carveOut(static_cast<char*>(out.block));
     }
     if (n > 0)
     {
@@ -552,9 +560,9 @@ done:
 }
 
 int build_mesh_gpu_indexed(const SoupIndexed& s, cudaStream_t stream, BuiltMesh& out, std::string& err, double* buildMs,
-                           long long* launchesOut, DeviceScratch* scratch)
+                           long long* launchesOut, DeviceScratch* scratch, DeviceScratch* upload)
 {
-    out.release();
+    out.reset();
     if (s.triCount < 0 || s.triCount > 0x7fffffff / 3)
     {
         err = "triangle count out of range";
@@ -578,7 +586,16 @@ int build_mesh_gpu_indexed(const SoupIndexed& s, cudaStream_t stream, BuiltMesh&
         return c.off;
     };
     char* block = nullptr;
-    cudaError_t e = dev_malloc(&block, carve(nullptr));
+    cudaError_t e = cudaSuccess;
+    if (upload)
+    {
+        e = upload->reserve(carve(nullptr));
+        block = static_cast<char*>(upload->p);
+    }
+    else
+    {
+        e = dev_malloc(&block, carve(nullptr));
+    }
     if (e == cudaSuccess) carve(block);
     if (e == cudaSuccess && s.nv) e = cudaMemcpyAsync(dv, s.v, sizeof(float) * 3 * (size_t)s.nv, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess && s.nvt)
@@ -603,7 +620,8 @@ int build_mesh_gpu_indexed(const SoupIndexed& s, cudaStream_t stream, BuiltMesh&
         status = build_mesh_gpu(reinterpret_cast<const prt_soup_triangle*>(dsoup), n, stream, out, err, buildMs,
                                 launchesOut, true, scratch);
     }
-    cudaFree(block);
+    if (!upload) cudaFree(block);
+    if (status != PRT_OK) out.release();
     return status;
 }
 

@@ -62,6 +62,7 @@ struct prt_ctx
     // acceleration structure
     Bvh8Device bvh;
     DeviceScratch buildScratch;   // BVH and mesh build scratch, reused by later builds
+    DeviceScratch uploadScratch;  // a parsed OBJ's lists on the device, reused by later mesh builds
     bool built = false;
     int leafMax = kDefaultLeafMax;
     bool highQuality = true;   // SAH grouping into 8-wide nodes
@@ -655,6 +656,7 @@ prt_ctx::~prt_ctx()
     clear_graphs(this);
     bvh.release();
     buildScratch.release();
+    uploadScratch.release();
     cudaFree(dPos);
     cudaFree(dIdx);
     cudaFree(dAlbedo);
@@ -1496,7 +1498,7 @@ int prt_build_mesh_soup(prt_ctx* ctx, const prt_soup* soup, prt_mesh_info* info)
     const auto t0 = std::chrono::steady_clock::now();
     double buildMs = 0;
     int st = build_mesh_gpu_indexed(s, ctx->stream, ctx->builtMesh, ctx->err, &buildMs, &ctx->launches,
-                                    &ctx->buildScratch);
+                                    &ctx->buildScratch, &ctx->uploadScratch);
     if (st != PRT_OK) return st;
     const auto t1 = std::chrono::steady_clock::now();
     BuiltMesh& m = ctx->builtMesh;

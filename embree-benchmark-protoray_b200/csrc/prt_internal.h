@@ -136,7 +136,8 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t* sums, int n,
 // An indexed mesh built from a triangle soup on the device (mesh_build.cu).
 struct BuiltMesh
 {
-    void* block = nullptr;  // the allocation holding idx, mat and attr
+    void* block = nullptr;  // the allocation holding idx, mat and attr (kept by the next build if large enough)
+    size_t blockBytes = 0;
     int* idx = nullptr;     // [3 * triCount]
     int* mat = nullptr;     // [triCount]
     float* attr = nullptr;  // [vertCount * stride]: position [, normal] [, texcoord], as in the .mesh blob
@@ -146,15 +147,21 @@ struct BuiltMesh
     std::vector<std::string> names;
     bool valid = false;
 
-    void release()
+    // forget the mesh, keep the allocation
+    void reset()
     {
-        if (block) cudaFree(block);
-        block = nullptr;
         idx = mat = nullptr;
         attr = nullptr;
         triCount = vertCount = 0;
         valid = false;
         names.clear();
+    }
+    void release()
+    {
+        reset();
+        if (block) cudaFree(block);
+        block = nullptr;
+        blockBytes = 0;
     }
 };
 
@@ -166,8 +173,10 @@ int build_mesh_gpu(const prt_soup_triangle* hostTris, int n, cudaStream_t stream
                    double* buildMs, long long* launches, bool soupOnDevice = false, DeviceScratch* scratch = nullptr);
 // The same for a parsed OBJ soup: uploads its indexed form and expands the
 // triangle records on the device.
+// upload: kept by the caller for the uploaded lists, or nullptr for a temporary block.
 int build_mesh_gpu_indexed(const SoupIndexed& soup, cudaStream_t stream, BuiltMesh& out, std::string& err,
-                           double* buildMs, long long* launches, DeviceScratch* scratch = nullptr);
+                           double* buildMs, long long* launches, DeviceScratch* scratch = nullptr,
+                           DeviceScratch* upload = nullptr);
 
 // Arguments of one wave of the wavefront renderer.
 struct WaveArgs

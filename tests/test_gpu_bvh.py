@@ -125,3 +125,36 @@ def test_build_quality_changes_grouping_not_hits(small):
         c._check(c.L.prt_set_build_quality(c.h, 2), "prt_set_build_quality")
     c.close()
 
+
+
+def test_rebuilds_reuse_scratch(small):
+    """A context keeps its build scratch between builds: rebuilding other
+    meshes of other sizes in one context gives the same trees (node count,
+    levels) and images as fresh contexts."""
+    import prt
+    import scenes
+    W, H = 64, 48
+    big, bview = scenes.batch_scene(5)
+    mesh, view = small
+
+    def run(c, m, v):
+        c.load_mesh(m.indices, m.positions)
+        st = c.build()
+        c.init_frame(W, H)
+        c.set_view(v, W, H)
+        c.render(2, 4, accumulate=False)
+        return st["nodeCount"], st["levels"], c.read_accum().copy()
+
+    fresh = {}
+    for name, m, v in (("small", mesh, view), ("big", big, bview)):
+        c = prt.Context(0)
+        fresh[name] = run(c, m, v)
+        c.close()
+    c = prt.Context(0)
+    for name, m, v in (("big", big, bview), ("small", mesh, view), ("big", big, bview), ("small", mesh, view)):
+        nodes, levels, img = run(c, m, v)
+        assert (nodes, levels) == fresh[name][:2], name
+        ref = fresh[name][2]
+        assert float(np.mean(np.abs(img[..., 0] - ref[..., 0]) / np.maximum(ref[..., 0], 1e-2))) < 1e-5, name
+        assert np.array_equal(img[..., 3], ref[..., 3]), name
+    c.close()

@@ -143,6 +143,8 @@ enum { PRT_INTEGRATOR_DIFFUSE = 0, PRT_INTEGRATOR_DIFFUSE2 = 1 };
 int prt_set_integrator(prt_ctx* ctx, int integrator);
 
 /* --- acceleration structure (OptixIntersectorStreamCuda ctor, accel/optix/optix_intersector_stream_cuda.cpp:23-75) --- */
+/* The context keeps the build's device scratch (about 160 bytes per triangle)
+ * for its later builds and mesh builds; prt_destroy frees it. */
 int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats);
 /* Largest leaf of the 8-wide tree, 1..3 triangles, for the next build. */
 int prt_set_leaf_size(prt_ctx* ctx, int maxTrianglesPerLeaf);
@@ -321,6 +323,9 @@ int prt_build_mesh(prt_ctx* ctx, const prt_soup_triangle* tris, int triCount, co
  * triangle's corner indices: 12 bytes per triangle plus 12 per vertex for a
  * positions-only file, instead of 100 per triangle) and expands it on the GPU. */
 int prt_build_mesh_soup(prt_ctx* ctx, const prt_soup* soup, prt_mesh_info* info);
+/* Both mesh builders keep their device buffers (the uploaded lists, the
+ * scratch, the built mesh's block) in the context for the next mesh build,
+ * which allocates only when it needs more; prt_destroy frees them. */
 /* Copies the built mesh to host arrays: indices[3*triCount],
  * materialIds[triCount], positions[3*vertCount]; normals[3*vertCount] and
  * texcoords[2*vertCount] only when present (else pass NULL). */

@@ -594,12 +594,25 @@ def main():
     rays_all = sum_over_ranks(rays, dist, dev)
     value = rays_all / 1e6 / (ms_max / 1e3)
 
-    # end-to-end through the C ABI with host buffers: camera in, image out
+    # end-to-end through the C ABI with host buffers: camera in, image out.
+    # With N ranks the frame is the sum of the ranks' accumulators (their
+    # pass ranges are disjoint): one NCCL reduce into rank 0, which reads it.
     host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    dev_img = torch.empty((H, W, 4), dtype=torch.float32, device=dev) if dist else None
     cam = prt.camera_from_view(view, W, H)
+
+    def frame_out():
+        if dist is None:
+            ctx.read_accum(host_img)
+            return
+        ctx.read_accum(dev_img)
+        dist.reduce(dev_img, dst=0, op=dist.ReduceOp.SUM)
+        if rank == 0:
+            host_img.copy_(dev_img)
+
     ctx.set_camera(cam)
     step(pass0)
-    ctx.read_accum(host_img)
+    frame_out()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -608,7 +621,7 @@ def main():
     for s in range(args.steps):
         ctx.set_camera(cam)
         st = step(pass0)
-        ctx.read_accum(host_img)
+        frame_out()
         e_rays += st["ray"]
     torch.cuda.synchronize()
     e_secs = max_over_ranks(time.perf_counter() - t0, dist, dev)

@@ -194,6 +194,383 @@ __global__ void k_karras(const uint32_t* __restrict__ keys, int n, int2* __restr
     if (i == 0) parent[0] = -1;
 }
 
+// --- 4b. SAH rebuild of the LBVH's small subtrees -----------------------------
+//
+// The Morton hierarchy splits space at fixed cell boundaries; below
+// kSahLeaves triangles the tree is rebuilt with an exact sweep SAH instead: a
+// maximal LBVH subtree of 2..kSahLeaves triangles covers a contiguous range
+// [a, b] of the sorted triangles, one block rebuilds it top-down (all nodes of
+// a depth at once), reusing the subtree's internal node indices and permuting
+// the triangles only inside [a, b], so the rest of the tree, the ranges and
+// the later passes are unchanged.  Splits: for each axis the range's
+// triangles sorted by centroid, the split after position p costs
+// area(left box) x |left| + area(right box) x |right|; the least cost wins
+// (ties to the more balanced split, then the lower axis and position).
+#ifndef PRT_SAH_REBUILD
+#define PRT_SAH_REBUILD 1
+#endif
+constexpr int kSahLeaves = 256;
+
+__device__ __forceinline__ int ref_size(const int2* range, int ref)
+{
+    if (ref < 0) return 1;
+    const int2 r = range[ref];
+    return r.y - r.x + 1;
+}
+
+// Roots of the subtrees to rebuild: internal nodes of 2..kSahLeaves triangles
+// whose parent has more (or that are the tree's root).
+__global__ void k_sah_roots(int n, const int2* __restrict__ range, const int* __restrict__ parent, int* roots,
+                            int* numRoots)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n - 1) return;
+    const int s = ref_size(range, u);
+    if (s > kSahLeaves) return;
+    const int p = parent[u];
+    if (p >= 0 && ref_size(range, p) <= kSahLeaves) return;
+    roots[atomicAdd(numRoots, 1)] = u;
+}
+
+// The internal nodes of each subtree, listed at slots[a ..] for the subtree
+// whose range starts at a (slotCount[a] zeroed).
+__global__ void k_sah_slots(int n, const int2* __restrict__ range, const int* __restrict__ parent, int* slots,
+                            int* slotCount)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n - 1) return;
+    if (ref_size(range, u) > kSahLeaves) return;
+    int r = u;
+    for (int p = parent[r]; p >= 0 && ref_size(range, p) <= kSahLeaves; p = parent[r]) r = p;
+    const int a = range[r].x;
+    slots[a + atomicAdd(slotCount + a, 1)] = u;
+}
+
+struct SahShared
+{
+    float box[6][kSahLeaves];         // triangle boxes of the range (lo xyz, hi xyz)
+    float cen[3][kSahLeaves];         // doubled centroids
+    int list[2][3][kSahLeaves];       // per axis: elements in centroid order (double buffered)
+    float scan[6][kSahLeaves];        // prefix / suffix boxes of one axis list
+    float preArea[kSahLeaves];        // area of the prefix box ending at each position
+    unsigned long long best[kSahLeaves];   // per segment: least split key
+    int segStart[kSahLeaves], segEnd[kSahLeaves], segNode[kSahLeaves], segRight[kSahLeaves];
+    int segOf[kSahLeaves];            // per position: its segment
+    int rank[3][kSahLeaves];          // segmented scan of the left marks, per axis list
+    int orig[kSahLeaves];             // triangle id of each element
+    int pool[kSahLeaves];             // internal node indices of the subtree (root first)
+    unsigned char mark[kSahLeaves];   // element goes left
+    int nseg, poolNext, splitting, rootPos;
+    int maxSeg, nextMaxSeg;   // largest segment of this depth / of the next
+};
+
+__device__ __forceinline__ float area6(float lx, float ly, float lz, float hx, float hy, float hz)
+{
+    const float dx = hx - lx, dy = hy - ly, dz = hz - lz;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __restrict__ roots,
+                                                          const int* __restrict__ numRoots,
+                                                          const float* __restrict__ triBox, uint32_t* vals,
+                                                          int2* child, int2* range, int* parent,
+                                                          const int* __restrict__ slots)
+{
+    __shared__ SahShared S;
+    const int t = threadIdx.x;
+    const int count = *numRoots;
+    for (int ri = blockIdx.x; ri < count; ri += gridDim.x)
+    {
+        const int u = roots[ri];
+        const int2 rg = range[u];
+        const int a = rg.x, ns = rg.y - rg.x + 1;   // 2 <= ns <= kSahLeaves
+        // --- load the range ---------------------------------------------------
+        if (t < ns)
+        {
+            const uint32_t tri = vals[a + t];
+            S.orig[t] = (int)tri;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) S.box[k][t] = triBox[6 * (size_t)tri + k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) S.cen[k][t] = S.box[k][t] + S.box[3 + k][t];
+            S.segOf[t] = 0;
+        }
+        if (t < ns - 1)
+        {
+            const int v = slots[a + t];
+            S.pool[t] = v;
+            if (v == u) S.rootPos = t;
+        }
+        if (t == 0)
+        {
+            S.nseg = 1;
+            S.segStart[0] = 0;
+            S.segEnd[0] = ns - 1;
+            S.poolNext = 1;
+        }
+        __syncthreads();
+        if (t == 0)
+        {
+            const int rp = S.rootPos;
+            S.pool[rp] = S.pool[0];
+            S.pool[0] = u;
+            S.segNode[0] = u;
+        }
+        // --- per axis: elements sorted by centroid (bitonic, ties by element;
+        //     the three axes side by side) ---------------------------------------
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax)
+        {
+            S.scan[ax][t] = t < ns ? S.cen[ax][t] : FLT_MAX;
+            S.list[0][ax][t] = t < ns ? t : kSahLeaves + t;
+        }
+        __syncthreads();
+        for (int size = 2; size <= kSahLeaves; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1)
+            {
+                const int o = t ^ stride;
+                const bool up = (t & size) == 0;
+                const bool lower = t < o;
+                float ko[3];
+                int io[3];
+                bool take[3];
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax)
+                {
+                    ko[ax] = S.scan[ax][o];
+                    io[ax] = S.list[0][ax][o];
+                    const float km = S.scan[ax][t];
+                    const int im = S.list[0][ax][t];
+                    const bool mGreater = km > ko[ax] || (km == ko[ax] && im > io[ax]);
+                    take[ax] = lower ? (up ? mGreater : !mGreater) : (up ? !mGreater : mGreater);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax)
+                    if (take[ax])
+                    {
+                        S.scan[ax][t] = ko[ax];
+                        S.list[0][ax][t] = io[ax];
+                    }
+                __syncthreads();
+            }
+        int cur = 0;
+        if (t == 0)
+        {
+            S.splitting = 0;
+            S.maxSeg = ns;
+        }
+        __syncthreads();
+        // --- one depth of the subtree per pass -------------------------------------
+        for (int depth = 0; depth < kSahLeaves; ++depth)
+        {
+            if (t < S.nseg)
+            {
+                S.best[t] = ~0ull;
+                if (S.segEnd[t] > S.segStart[t]) S.splitting = 1;
+            }
+            __syncthreads();
+            if (!S.splitting) break;
+            const int s = t < ns ? S.segOf[t] : 0;
+            const int st0 = t < ns ? S.segStart[s] : 0, en0 = t < ns ? S.segEnd[s] : 0;
+            const int span = S.maxSeg;   // scans within segments need log2(span) steps
+            if (t == 0) S.nextMaxSeg = 1;
+            for (int ax = 0; ax < 3; ++ax)
+            {
+                // prefix boxes along the axis list, within segments
+                float v[6];
+                if (t < ns)
+                {
+                    const int e = S.list[cur][ax][t];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) v[k] = S.box[k][e];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) S.scan[k][t] = v[k];
+                }
+                __syncthreads();
+                for (int off = 1; off < span; off <<= 1)
+                {
+                    const bool take = t < ns && t - off >= st0;
+                    float w[6];
+                    if (take)
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) w[k] = S.scan[k][t - off];
+                    __syncthreads();
+                    if (take)
+                    {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                        {
+                            v[k] = fminf(v[k], w[k]);
+                            v[3 + k] = fmaxf(v[3 + k], w[3 + k]);
+                            S.scan[k][t] = v[k];
+                            S.scan[3 + k][t] = v[3 + k];
+                        }
+                    }
+                    __syncthreads();
+                }
+                if (t < ns) S.preArea[t] = area6(v[0], v[1], v[2], v[3], v[4], v[5]);
+                // suffix boxes
+                if (t < ns)
+                {
+                    const int e = S.list[cur][ax][t];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) v[k] = S.box[k][e];
+                }
+                __syncthreads();
+                if (t < ns)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) S.scan[k][t] = v[k];
+                __syncthreads();
+                for (int off = 1; off < span; off <<= 1)
+                {
+                    const bool take = t < ns && t + off <= en0;
+                    float w[6];
+                    if (take)
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) w[k] = S.scan[k][t + off];
+                    __syncthreads();
+                    if (take)
+                    {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                        {
+                            v[k] = fminf(v[k], w[k]);
+                            v[3 + k] = fmaxf(v[3 + k], w[3 + k]);
+                            S.scan[k][t] = v[k];
+                            S.scan[3 + k][t] = v[3 + k];
+                        }
+                    }
+                    __syncthreads();
+                }
+                // cost of the split after position t (the suffix from t + 1)
+                if (t < ns && t < en0)
+                {
+                    const float sa = area6(S.scan[0][t + 1], S.scan[1][t + 1], S.scan[2][t + 1], S.scan[3][t + 1],
+                                           S.scan[4][t + 1], S.scan[5][t + 1]);
+                    const int nl = t - st0 + 1, nr = en0 - t;
+                    const float c = S.preArea[t] * (float)nl + sa * (float)nr;
+                    const unsigned imbalance = (unsigned)abs(nl - nr);
+                    const unsigned long long key = ((unsigned long long)__float_as_uint(fmaxf(c, 0.f)) << 32) |
+                                                   ((unsigned long long)imbalance << 16) | ((unsigned)ax << 8) |
+                                                   (unsigned)(t - st0);
+                    atomicMin(&S.best[s], key);
+                }
+                __syncthreads();
+            }
+            // marks: the chosen axis list's prefix goes left
+            if (t < ns && en0 > st0)
+            {
+                const unsigned long long b = S.best[s];
+                const int ax = (int)((b >> 8) & 0xff), sp = st0 + (int)(b & 0xff);
+                S.mark[S.list[cur][ax][t]] = t <= sp ? 1 : 0;
+            }
+            __syncthreads();
+            // stable partition of the three lists within the splitting segments
+            int m[3] = {0, 0, 0};
+            if (t < ns && en0 > st0)
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax) m[ax] = S.mark[S.list[cur][ax][t]];
+            int incl[3] = {m[0], m[1], m[2]};
+            if (t < ns)
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax) S.rank[ax][t] = incl[ax];
+            __syncthreads();
+            for (int off = 1; off < span; off <<= 1)
+            {
+                const bool take = t < ns && t - off >= st0;
+                int w[3] = {0, 0, 0};
+                if (take)
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) w[ax] = S.rank[ax][t - off];
+                __syncthreads();
+                if (take)
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax)
+                    {
+                        incl[ax] += w[ax];
+                        S.rank[ax][t] = incl[ax];
+                    }
+                __syncthreads();
+            }
+            if (t < ns)
+            {
+                if (en0 > st0)
+                {
+                    const unsigned long long b = S.best[s];
+                    const int nl = (int)(b & 0xff) + 1;
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax)
+                    {
+                        const int before = incl[ax] - m[ax];   // left elements before t in the segment
+                        const int np = m[ax] ? st0 + before : st0 + nl + (t - st0 - before);
+                        S.list[cur ^ 1][ax][np] = S.list[cur][ax][t];
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) S.list[cur ^ 1][ax][t] = S.list[cur][ax][t];
+                }
+            }
+            __syncthreads();
+            // nodes: each splitting segment is an internal node with two children
+            const int nsegOld = S.nseg;
+            __syncthreads();
+            if (t < nsegOld && S.segEnd[t] > S.segStart[t])
+            {
+                const int st = S.segStart[t], en = S.segEnd[t], node = S.segNode[t];
+                const int sp = st + (int)(S.best[t] & 0xff);
+                int refs[2];
+                const int cs[2] = {st, sp + 1}, ce[2] = {sp, en};
+                const int right = atomicAdd(&S.nseg, 1);
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                {
+                    const int segId = c == 0 ? t : right;
+                    if (ce[c] == cs[c])
+                    {
+                        refs[c] = ~(a + cs[c]);
+                        parent[(n - 1) + a + cs[c]] = node;
+                        S.segNode[segId] = -1;
+                    }
+                    else
+                    {
+                        const int id = S.pool[atomicAdd(&S.poolNext, 1)];
+                        refs[c] = id;
+                        parent[id] = node;
+                        range[id] = make_int2(a + cs[c], a + ce[c]);
+                        S.segNode[segId] = id;
+                    }
+                }
+                child[node] = make_int2(refs[0], refs[1]);
+                atomicMax(&S.nextMaxSeg, max(sp - st + 1, en - sp));
+                S.segRight[t] = right;
+                S.segStart[right] = sp + 1;
+                S.segEnd[right] = en;
+                S.segEnd[t] = sp;
+            }
+            __syncthreads();
+            if (t < ns && en0 > st0)
+            {
+                const unsigned long long b = S.best[s];
+                const int sp = st0 + (int)(b & 0xff);
+                if (t > sp) S.segOf[t] = S.segRight[s];
+            }
+            if (t == 0)
+            {
+                S.splitting = 0;
+                S.maxSeg = S.nextMaxSeg;
+            }
+            cur ^= 1;
+            __syncthreads();
+        }
+        // the triangles in their new order
+        if (t < ns) vals[a + t] = (uint32_t)S.orig[S.list[cur][0][t]];
+        __syncthreads();
+    }
+}
+
 // --- 5. bottom-up refit and SAH-optimal grouping into 8-wide nodes ----------
 //
 // One thread per triangle walks up the tree; the second thread to arrive at
@@ -928,6 +1305,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     const int boundBlocks = std::min(1024, div_up(n, 256));
     const int nodeCapacity = std::max(1, nInternal);
     const bool group = PRT_WIDE_DP && sahGrouping && nInternal > 0;
+    const bool rebuild = PRT_SAH_REBUILD && sahGrouping && nInternal > 0;
     int device = 0, numSMs = 148;
     if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device);
 
@@ -935,7 +1313,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     float *triBox, *partial, *cbounds, *box;
     uint32_t *keysA, *keysB, *valsA, *valsB, *hist;
     int2 *child, *range;
-    int *parent, *flag, *collapseErr, *marks, *binRef;
+    int *parent, *flag, *collapseErr, *marks, *binRef, *sahRoots, *sahSlots, *sahCount;
     unsigned long long* collapseAlloc;
     float4* dpCost;
     uint2* dpDec;
@@ -955,6 +1333,9 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         flag = c.take<int>(nodeCapacity);
         box = c.take<float>(6 * (size_t)(2 * n));
         binRef = c.take<int>(nodeCapacity);
+        sahRoots = rebuild ? c.take<int>(nodeCapacity) : nullptr;
+        sahSlots = rebuild ? c.take<int>(n) : nullptr;
+        sahCount = rebuild ? c.take<int>((size_t)n + 1) : nullptr;
         collapseAlloc = c.take<unsigned long long>(1);
         collapseErr = c.take<int>(1);
         marks = c.take<int>(kCollapseLevels + 2);
@@ -998,6 +1379,18 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     {
         k_karras<<<div_up(nInternal, 256), 256, 0, stream>>>(keysA, n, child, range, parent);
         BUILD_CHECK(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)nInternal, stream));
+        if (rebuild)
+        {
+            // sahCount[0..n): slots per subtree start, sahCount[n]: roots
+            BUILD_CHECK(cudaMemsetAsync(sahCount, 0, sizeof(int) * ((size_t)n + 1), stream));
+            k_sah_roots<<<div_up(nInternal, 256), 256, 0, stream>>>(n, range, parent, sahRoots, sahCount + n);
+            k_sah_slots<<<div_up(nInternal, 256), 256, 0, stream>>>(n, range, parent, sahSlots, sahCount);
+            int perSM = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_sah_rebuild, kSahLeaves, 0);
+            k_sah_rebuild<<<std::max(1, perSM) * numSMs, kSahLeaves, 0, stream>>>(n, sahRoots, sahCount + n, triBox,
+                                                                               valsA, child, range, parent, sahSlots);
+            BUILD_CHECK(cudaGetLastError());
+        }
     }
     else
     {

@@ -32,6 +32,8 @@ namespace prt_b200 {
 
 namespace {
 
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
 struct Box6
 {
     float lo[3], hi[3];
@@ -194,57 +196,25 @@ __global__ void k_karras(const uint32_t* __restrict__ keys, int n, int2* __restr
     if (i == 0) parent[0] = -1;
 }
 
-// --- 4b. SAH rebuild of the LBVH's small subtrees -----------------------------
+__device__ __forceinline__ float box_half_area_lh(const float* lo, const float* hi)
+{
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// --- 4b. exact sweep SAH for subtrees of at most kSahLeaves triangles ---------
 //
-// The Morton hierarchy splits space at fixed cell boundaries; below
-// kSahLeaves triangles the tree is rebuilt with an exact sweep SAH instead: a
-// maximal LBVH subtree of 2..kSahLeaves triangles covers a contiguous range
-// [a, b] of the sorted triangles, one block rebuilds it top-down (all nodes of
-// a depth at once), reusing the subtree's internal node indices and permuting
-// the triangles only inside [a, b], so the rest of the tree, the ranges and
-// the later passes are unchanged.  Splits: for each axis the range's
-// triangles sorted by centroid, the split after position p costs
-// area(left box) x |left| + area(right box) x |right|; the least cost wins
-// (ties to the more balanced split, then the lower axis and position).
-#ifndef PRT_SAH_REBUILD
-#define PRT_SAH_REBUILD 1
+// A subtree of 2..kSahLeaves triangles covers a contiguous range [a, b] of the
+// triangle order; one block builds it top-down to single-triangle leaves, all
+// nodes of a depth at once, permuting the triangles only inside [a, b].
+// Splits: for each axis the range's triangles sorted by centroid, the split
+// after position p costs area(left box) x |left| + area(right box) x |right|;
+// the least cost wins (ties to the more balanced split, then the lower axis
+// and position).
+#ifndef PRT_SAH_BUILD
+#define PRT_SAH_BUILD 1
 #endif
 constexpr int kSahLeaves = 256;
-
-__device__ __forceinline__ int ref_size(const int2* range, int ref)
-{
-    if (ref < 0) return 1;
-    const int2 r = range[ref];
-    return r.y - r.x + 1;
-}
-
-// Roots of the subtrees to rebuild: internal nodes of 2..kSahLeaves triangles
-// whose parent has more (or that are the tree's root).
-__global__ void k_sah_roots(int n, const int2* __restrict__ range, const int* __restrict__ parent, int* roots,
-                            int* numRoots)
-{
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= n - 1) return;
-    const int s = ref_size(range, u);
-    if (s > kSahLeaves) return;
-    const int p = parent[u];
-    if (p >= 0 && ref_size(range, p) <= kSahLeaves) return;
-    roots[atomicAdd(numRoots, 1)] = u;
-}
-
-// The internal nodes of each subtree, listed at slots[a ..] for the subtree
-// whose range starts at a (slotCount[a] zeroed).
-__global__ void k_sah_slots(int n, const int2* __restrict__ range, const int* __restrict__ parent, int* slots,
-                            int* slotCount)
-{
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= n - 1) return;
-    if (ref_size(range, u) > kSahLeaves) return;
-    int r = u;
-    for (int p = parent[r]; p >= 0 && ref_size(range, p) <= kSahLeaves; p = parent[r]) r = p;
-    const int a = range[r].x;
-    slots[a + atomicAdd(slotCount + a, 1)] = u;
-}
 
 struct SahShared
 {
@@ -260,7 +230,7 @@ struct SahShared
     int orig[kSahLeaves];             // triangle id of each element
     int pool[kSahLeaves];             // internal node indices of the subtree (root first)
     unsigned char mark[kSahLeaves];   // element goes left
-    int nseg, poolNext, splitting, rootPos;
+    int nseg, poolNext, splitting, rootPos;   // rootPos: the first new node index
     int maxSeg, nextMaxSeg;   // largest segment of this depth / of the next
 };
 
@@ -270,11 +240,13 @@ __device__ __forceinline__ float area6(float lx, float ly, float lz, float hx, f
     return dx * dy + dy * dz + dz * dx;
 }
 
+// One subtree per block: roots[i] is its root (an internal node whose range
+// holds 2..kSahLeaves triangles); its other internal nodes take new indices
+// from *nodeCounter.
 __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __restrict__ roots,
                                                           const int* __restrict__ numRoots,
                                                           const float* __restrict__ triBox, uint32_t* vals,
-                                                          int2* child, int2* range, int* parent,
-                                                          const int* __restrict__ slots)
+                                                          int2* child, int2* range, int* parent, int* nodeCounter)
 {
     __shared__ SahShared S;
     const int t = threadIdx.x;
@@ -284,6 +256,7 @@ __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __
         const int u = roots[ri];
         const int2 rg = range[u];
         const int a = rg.x, ns = rg.y - rg.x + 1;   // 2 <= ns <= kSahLeaves
+        if (t == 0) S.rootPos = ns > 2 ? atomicAdd(nodeCounter, ns - 2) : 0;   // first new index
         // --- load the range ---------------------------------------------------
         if (t < ns)
         {
@@ -295,12 +268,6 @@ __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __
             for (int k = 0; k < 3; ++k) S.cen[k][t] = S.box[k][t] + S.box[3 + k][t];
             S.segOf[t] = 0;
         }
-        if (t < ns - 1)
-        {
-            const int v = slots[a + t];
-            S.pool[t] = v;
-            if (v == u) S.rootPos = t;
-        }
         if (t == 0)
         {
             S.nseg = 1;
@@ -309,13 +276,8 @@ __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __
             S.poolNext = 1;
         }
         __syncthreads();
-        if (t == 0)
-        {
-            const int rp = S.rootPos;
-            S.pool[rp] = S.pool[0];
-            S.pool[0] = u;
-            S.segNode[0] = u;
-        }
+        if (t < ns - 1) S.pool[t] = t == 0 ? u : S.rootPos + t - 1;
+        if (t == 0) S.segNode[0] = u;
         // --- per axis: elements sorted by centroid (bitonic, ties by element;
         //     the three axes side by side) ---------------------------------------
 #pragma unroll
@@ -569,6 +531,480 @@ __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __
         if (t < ns) vals[a + t] = (uint32_t)S.orig[S.list[cur][0][t]];
         __syncthreads();
     }
+}
+
+// --- 4c. top-down binned SAH above kSahLeaves triangles ------------------------
+//
+// The high-quality build does not use the Morton hierarchy's top either: from
+// the root, every task (a node and its contiguous range of triangles) with
+// more than kSahLeaves triangles is split by the least SAH cost over
+// kTopBins centroid bins per axis (bin boxes and counts gathered per chunk of
+// the range in shared memory, then merged with atomics), its triangles are
+// partitioned into the two halves of the range, and the halves become the
+// next level's tasks, k_sah_rebuild's subtrees (2..kSahLeaves triangles) or
+// leaves.  One host read-back per level sizes the next level's launches.
+constexpr int kTopBins = 32;
+constexpr int kTopChunk = 4096;        // triangles per block of the binning and partition passes
+constexpr int kBinWords = 13;          // count, box lo/hi, centroid lo/hi (order-preserving float bits)
+
+struct TopTask
+{
+    int lo, hi, node, pad;
+    float cmin[3], cmax[3];   // centroid bounds
+};
+
+struct TopSplit
+{
+    int axis;       // -1: no bin separates the centroids; split the range in the middle
+    int bin;        // left: bins 0..bin
+    int nl;         // triangles going left
+    int pad;
+};
+
+__device__ __forceinline__ uint32_t ford(float f)
+{
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float funord(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__device__ __forceinline__ int top_bin(float c, float cmin, float scale)
+{
+    return min(kTopBins - 1, max(0, (int)((c - cmin) * scale)));
+}
+
+__device__ __forceinline__ float top_scale(float cmin, float cmax)
+{
+    const float e = cmax - cmin;
+    return e > 0.f ? (float)kTopBins * 0.99999f / e : 0.f;
+}
+
+__global__ void k_top_init_bins(uint32_t* bins, int words)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x)
+    {
+        const int w = i % kBinWords;
+        // count 0; lo fields (1-3, 7-9) start at the largest value, hi fields at 0
+        bins[i] = w == 0 ? 0u : (((w >= 1 && w <= 3) || (w >= 7 && w <= 9)) ? 0xffffffffu : 0u);
+    }
+}
+
+// Chunk c: task chunks[c].x, triangles [chunks[c].y, chunks[c].z].
+__global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks, const TopTask* __restrict__ tasks,
+                                                 const uint32_t* __restrict__ perm, const float* __restrict__ triBox,
+                                                 uint32_t* bins)
+{
+    __shared__ uint32_t sb[3 * kTopBins * kBinWords];
+    const int4 ch = chunks[blockIdx.x];
+    const TopTask tk = tasks[ch.x];
+    for (int i = threadIdx.x; i < 3 * kTopBins * kBinWords; i += blockDim.x)
+    {
+        const int w = i % kBinWords;
+        sb[i] = w == 0 ? 0u : (((w >= 1 && w <= 3) || (w >= 7 && w <= 9)) ? 0xffffffffu : 0u);
+    }
+    __syncthreads();
+    float sc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sc[k] = top_scale(tk.cmin[k], tk.cmax[k]);
+    const unsigned lane = threadIdx.x & 31u;
+    for (int i0 = ch.y; i0 <= ch.z; i0 += blockDim.x)
+    {
+        // the lanes of a warp that fall into one bin (neighbours in the
+        // triangle order often do) merge their boxes with warp reductions and
+        // one lane updates the bin
+        const int i = i0 + threadIdx.x;
+        const bool valid = i <= ch.z;
+        uint32_t lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0, 0, 0};
+        uint32_t cq[3] = {0, 0, 0};
+        float c[3] = {0.f, 0.f, 0.f};
+        if (valid)
+        {
+            const uint32_t tri = perm[i];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                const float bl = triBox[6 * (size_t)tri + k], bh = triBox[6 * (size_t)tri + 3 + k];
+                lo[k] = ford(bl);
+                hi[k] = ford(bh);
+                c[k] = 0.5f * (bl + bh);
+                cq[k] = ford(c[k]);
+            }
+        }
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax)
+        {
+            const int bin = valid ? top_bin(c[ax], tk.cmin[ax], sc[ax]) : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, bin);
+            uint32_t r[13];
+            r[0] = __popc(peers);
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                r[1 + k] = __reduce_min_sync(peers, lo[k]);
+                r[4 + k] = __reduce_max_sync(peers, hi[k]);
+                r[7 + k] = __reduce_min_sync(peers, cq[k]);
+                r[10 + k] = __reduce_max_sync(peers, cq[k]);
+            }
+            if (valid && lane == (unsigned)(__ffs(peers) - 1))
+            {
+                uint32_t* w = sb + (ax * kTopBins + bin) * kBinWords;
+                atomicAdd(w, r[0]);
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    atomicMin(w + 1 + k, r[1 + k]);
+                    atomicMax(w + 4 + k, r[4 + k]);
+                    atomicMin(w + 7 + k, r[7 + k]);
+                    atomicMax(w + 10 + k, r[10 + k]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    uint32_t* g = bins + (size_t)ch.x * 3 * kTopBins * kBinWords;
+    for (int i = threadIdx.x; i < 3 * kTopBins * kBinWords; i += blockDim.x)
+    {
+        const int w = i % kBinWords;
+        if (w == 0)
+        {
+            if (sb[i]) atomicAdd(g + i, sb[i]);
+        }
+        else if ((w >= 1 && w <= 3) || (w >= 7 && w <= 9))
+        {
+            if (sb[i] != 0xffffffffu) atomicMin(g + i, sb[i]);
+        }
+        else if (sb[i])
+        {
+            atomicMax(g + i, sb[i]);
+        }
+    }
+}
+
+// One thread per task: the least-cost split over the bins of the three axes.
+__global__ void k_top_split(const TopTask* __restrict__ tasks, int numTasks, const uint32_t* __restrict__ bins,
+                            TopSplit* splits)
+{
+    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= numTasks) return;
+    const TopTask tk = tasks[ti];
+    const uint32_t* g = bins + (size_t)ti * 3 * kTopBins * kBinWords;
+    float best = FLT_MAX;
+    TopSplit sp{-1, 0, (tk.hi - tk.lo + 1) / 2, 0};
+    for (int ax = 0; ax < 3; ++ax)
+    {
+        float rArea[kTopBins];
+        int rCnt[kTopBins];
+        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        int cnt = 0;
+        for (int b = kTopBins - 1; b >= 0; --b)
+        {
+            const uint32_t* w = g + (ax * kTopBins + b) * kBinWords;
+            if (w[0])
+                for (int k = 0; k < 3; ++k)
+                {
+                    lo[k] = fminf(lo[k], funord(w[1 + k]));
+                    hi[k] = fmaxf(hi[k], funord(w[4 + k]));
+                }
+            cnt += (int)w[0];
+            rCnt[b] = cnt;
+            rArea[b] = cnt ? box_half_area_lh(lo, hi) : 0.f;
+        }
+        for (int k = 0; k < 3; ++k)
+        {
+            lo[k] = FLT_MAX;
+            hi[k] = -FLT_MAX;
+        }
+        cnt = 0;
+        for (int b = 0; b < kTopBins - 1; ++b)
+        {
+            const uint32_t* w = g + (ax * kTopBins + b) * kBinWords;
+            if (w[0])
+                for (int k = 0; k < 3; ++k)
+                {
+                    lo[k] = fminf(lo[k], funord(w[1 + k]));
+                    hi[k] = fmaxf(hi[k], funord(w[4 + k]));
+                }
+            cnt += (int)w[0];
+            if (cnt == 0 || rCnt[b + 1] == 0) continue;
+            const float c = box_half_area_lh(lo, hi) * (float)cnt + rArea[b + 1] * (float)rCnt[b + 1];
+            if (c < best)
+            {
+                best = c;
+                sp.axis = ax;
+                sp.bin = b;
+                sp.nl = cnt;
+            }
+        }
+    }
+    splits[ti] = sp;
+}
+
+// One thread per task: the two halves become internal nodes (next-level tasks
+// or rebuild subtrees) or leaves.
+__global__ void k_top_children(const TopTask* __restrict__ tasks, int numTasks, const TopSplit* __restrict__ splits,
+                               const uint32_t* __restrict__ bins, int n, TopTask* nextTasks, int* numNext,
+                               int* small, int* numSmall, int* nodeCounter, int2* child, int2* range, int* parent)
+{
+    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= numTasks) return;
+    const TopTask tk = tasks[ti];
+    const TopSplit sp = splits[ti];
+    const uint32_t* g = bins + (size_t)ti * 3 * kTopBins * kBinWords;
+    const int lo[2] = {tk.lo, tk.lo + sp.nl}, hi[2] = {tk.lo + sp.nl - 1, tk.hi};
+    int refs[2];
+    for (int side = 0; side < 2; ++side)
+    {
+        const int size = hi[side] - lo[side] + 1;
+        if (size == 1)
+        {
+            refs[side] = ~lo[side];
+            parent[(n - 1) + lo[side]] = tk.node;
+            continue;
+        }
+        const int id = atomicAdd(nodeCounter, 1);
+        refs[side] = id;
+        parent[id] = tk.node;
+        range[id] = make_int2(lo[side], hi[side]);
+        if (size <= kSahLeaves)
+        {
+            small[atomicAdd(numSmall, 1)] = id;
+            continue;
+        }
+        TopTask c;
+        c.lo = lo[side];
+        c.hi = hi[side];
+        c.node = id;
+        c.pad = 0;
+        if (sp.axis < 0)
+        {
+            for (int k = 0; k < 3; ++k)
+            {
+                c.cmin[k] = tk.cmin[k];
+                c.cmax[k] = tk.cmax[k];
+            }
+        }
+        else
+        {
+            for (int k = 0; k < 3; ++k)
+            {
+                c.cmin[k] = FLT_MAX;
+                c.cmax[k] = -FLT_MAX;
+            }
+            const int b0 = side == 0 ? 0 : sp.bin + 1, b1 = side == 0 ? sp.bin : kTopBins - 1;
+            for (int b = b0; b <= b1; ++b)
+            {
+                const uint32_t* w = g + (sp.axis * kTopBins + b) * kBinWords;
+                if (!w[0]) continue;
+                for (int k = 0; k < 3; ++k)
+                {
+                    c.cmin[k] = fminf(c.cmin[k], funord(w[7 + k]));
+                    c.cmax[k] = fmaxf(c.cmax[k], funord(w[10 + k]));
+                }
+            }
+        }
+        nextTasks[atomicAdd(numNext, 1)] = c;
+    }
+    child[tk.node] = make_int2(refs[0], refs[1]);
+}
+
+__device__ __forceinline__ int top_side(const TopTask& tk, const TopSplit& sp, float sc, int i, uint32_t tri,
+                                        const float* __restrict__ triBox)
+{
+    if (sp.axis < 0) return i - tk.lo < sp.nl ? 0 : 1;
+    const float c = 0.5f * (triBox[6 * (size_t)tri + sp.axis] + triBox[6 * (size_t)tri + 3 + sp.axis]);
+    return top_bin(c, tk.cmin[sp.axis], sc) <= sp.bin ? 0 : 1;
+}
+
+// Triangles of each chunk that go left.
+__global__ void __launch_bounds__(256) k_top_count(const int4* __restrict__ chunks, const TopTask* __restrict__ tasks,
+                                                   const TopSplit* __restrict__ splits,
+                                                   const uint32_t* __restrict__ perm,
+                                                   const float* __restrict__ triBox, uint32_t* leftCount)
+{
+    __shared__ int warpCount[8];
+    const int4 ch = chunks[blockIdx.x];
+    const TopTask tk = tasks[ch.x];
+    const TopSplit sp = splits[ch.x];
+    const float sc = sp.axis >= 0 ? top_scale(tk.cmin[sp.axis], tk.cmax[sp.axis]) : 0.f;
+    int mine = 0;
+    for (int i = ch.y + threadIdx.x; i <= ch.z; i += blockDim.x) mine += top_side(tk, sp, sc, i, perm[i], triBox) == 0;
+    mine = __reduce_add_sync(0xffffffffu, mine);
+    if ((threadIdx.x & 31) == 0) warpCount[threadIdx.x >> 5] = mine;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int tot = 0;
+        for (int w = 0; w < 8; ++w) tot += warpCount[w];
+        leftCount[blockIdx.x] = (uint32_t)tot;
+    }
+}
+
+// The triangles of each chunk to their half of the task's range (in tmp), in
+// their order: leftBase = the chunk's left triangles before it in its task
+// (exclusive scan of k_top_count's counts minus the scan at the task's first
+// chunk, chunks[c].w).
+__global__ void __launch_bounds__(256) k_top_partition(const int4* __restrict__ chunks,
+                                                       const TopTask* __restrict__ tasks,
+                                                       const TopSplit* __restrict__ splits,
+                                                       const uint32_t* __restrict__ perm,
+                                                       const float* __restrict__ triBox,
+                                                       const uint32_t* __restrict__ leftScan, uint32_t* tmp)
+{
+    __shared__ int warpCount[2][8];
+    const int4 ch = chunks[blockIdx.x];
+    const TopTask tk = tasks[ch.x];
+    const TopSplit sp = splits[ch.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float sc = sp.axis >= 0 ? top_scale(tk.cmin[sp.axis], tk.cmax[sp.axis]) : 0.f;
+    int base[2];
+    base[0] = (int)(leftScan[blockIdx.x] - leftScan[ch.w]);
+    base[1] = (ch.y - tk.lo) - base[0];
+    for (int i0 = ch.y; i0 <= ch.z; i0 += blockDim.x)
+    {
+        const int i = i0 + threadIdx.x;
+        const bool valid = i <= ch.z;
+        uint32_t tri = 0;
+        int side = 0;
+        if (valid)
+        {
+            tri = perm[i];
+            side = top_side(tk, sp, sc, i, tri, triBox);
+        }
+        const unsigned left = __ballot_sync(0xffffffffu, valid && side == 0);
+        const unsigned right = __ballot_sync(0xffffffffu, valid && side == 1);
+        if (lane == 0)
+        {
+            warpCount[0][warp] = __popc(left);
+            warpCount[1][warp] = __popc(right);
+        }
+        __syncthreads();
+        if (valid)
+        {
+            int before = 0;
+            for (int w = 0; w < warp; ++w) before += warpCount[side][w];
+            const unsigned m = side == 0 ? left : right;
+            const int r = base[side] + before + __popc(m & ((1u << lane) - 1u));
+            const int dst = side == 0 ? tk.lo + r : tk.lo + sp.nl + r;
+            if (dst <= tk.hi) tmp[dst] = tri;
+        }
+        int tl = 0, tr = 0;
+        for (int w = 0; w < 8; ++w)
+        {
+            tl += warpCount[0][w];
+            tr += warpCount[1][w];
+        }
+        base[0] += tl;
+        base[1] += tr;
+        __syncthreads();
+    }
+}
+
+__global__ void k_top_copy(const int4* __restrict__ chunks, const uint32_t* __restrict__ tmp, uint32_t* perm)
+{
+    const int4 ch = chunks[blockIdx.x];
+    for (int i = ch.y + threadIdx.x; i <= ch.z; i += blockDim.x) perm[i] = tmp[i];
+}
+
+// The root: node 0 over all n triangles, a task (n > kSahLeaves) or a rebuild
+// subtree.  counters: [0] next-level tasks, [1] rebuild subtrees, [2] nodes.
+__global__ void k_top_root(const float* __restrict__ cbounds, int n, TopTask* tasks, int* small, int* counters,
+                           int2* range, int* parent)
+{
+    range[0] = make_int2(0, n - 1);
+    parent[0] = -1;
+    counters[0] = 0;
+    counters[1] = 0;
+    counters[2] = 1;
+    if (n <= kSahLeaves)
+    {
+        small[0] = 0;
+        counters[1] = 1;
+        return;
+    }
+    TopTask t;
+    t.lo = 0;
+    t.hi = n - 1;
+    t.node = 0;
+    t.pad = 0;
+    for (int k = 0; k < 3; ++k)
+    {
+        t.cmin[k] = cbounds[k];
+        t.cmax[k] = cbounds[3 + k];
+    }
+    tasks[0] = t;
+}
+
+struct TopBuffers
+{
+    TopTask* task[2];
+    TopSplit* splits;
+    uint32_t* bins;
+    uint32_t* leftCount;   // per chunk, then its exclusive scan
+    uint32_t* scanSums;
+    int* small;
+    int* counters;
+    int4* chunks;
+    uint32_t* tmp;
+    int maxTasks, maxChunks;
+};
+
+// Top-down binned SAH from the root down to subtrees of kSahLeaves triangles,
+// then k_sah_rebuild for those.  perm: the triangles (reordered in place).
+cudaError_t sah_top_down(int n, const float* triBox, const float* cbounds, uint32_t* perm, int2* child, int2* range,
+                         int* parent, const TopBuffers& B, int numSMs, cudaStream_t stream)
+{
+    k_top_root<<<1, 1, 0, stream>>>(cbounds, n, B.task[0], B.small, B.counters, range, parent);
+    cudaError_t e = cudaGetLastError();
+    int numTasks = n > kSahLeaves ? 1 : 0;
+    int cur = 0;
+    std::vector<TopTask> host;
+    std::vector<int4> chunks;
+    while (e == cudaSuccess && numTasks > 0)
+    {
+        if (numTasks > B.maxTasks) return cudaErrorInvalidValue;
+        host.resize(numTasks);
+        e = cudaMemcpyAsync(host.data(), B.task[cur], sizeof(TopTask) * numTasks, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) break;
+        chunks.clear();
+        for (int ti = 0; ti < numTasks; ++ti)
+        {
+            const int first = (int)chunks.size();
+            for (int s = host[ti].lo; s <= host[ti].hi; s += kTopChunk)
+                chunks.push_back(make_int4(ti, s, std::min(host[ti].hi, s + kTopChunk - 1), first));
+        }
+        const int nch = (int)chunks.size();
+        if (nch > B.maxChunks) return cudaErrorInvalidValue;
+        e = cudaMemcpyAsync(B.chunks, chunks.data(), sizeof(int4) * nch, cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) break;
+        const int words = numTasks * 3 * kTopBins * kBinWords;
+        k_top_init_bins<<<std::min(div_up(words, 256), 4 * numSMs), 256, 0, stream>>>(B.bins, words);
+        k_top_bin<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], perm, triBox, B.bins);
+        k_top_split<<<div_up(numTasks, 128), 128, 0, stream>>>(B.task[cur], numTasks, B.bins, B.splits);
+        e = cudaMemsetAsync(B.counters, 0, sizeof(int), stream);
+        if (e != cudaSuccess) break;
+        k_top_children<<<div_up(numTasks, 128), 128, 0, stream>>>(B.task[cur], numTasks, B.splits, B.bins, n,
+                                                                   B.task[cur ^ 1], B.counters, B.small,
+                                                                   B.counters + 1, B.counters + 2, child, range,
+                                                                   parent);
+        k_top_count<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], B.splits, perm, triBox, B.leftCount);
+        exclusive_scan_u32(B.leftCount, B.leftCount, B.scanSums, nch, stream);
+        k_top_partition<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], B.splits, perm, triBox, B.leftCount, B.tmp);
+        k_top_copy<<<nch, 256, 0, stream>>>(B.chunks, B.tmp, perm);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&numTasks, B.counters, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        cur ^= 1;
+    }
+    if (e != cudaSuccess) return e;
+    int perSM = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_sah_rebuild, kSahLeaves, 0);
+    k_sah_rebuild<<<std::max(1, perSM) * numSMs, kSahLeaves, 0, stream>>>(n, B.small, B.counters + 1, triBox, perm,
+                                                                       child, range, parent, B.counters + 2);
+    return cudaGetLastError();
 }
 
 // --- 5. bottom-up refit and SAH-optimal grouping into 8-wide nodes ----------
@@ -1214,7 +1650,6 @@ __global__ void k_collapse_mark(CollapseArgs a, int level)
     a.marks[level + 2] = (int)(*(volatile unsigned long long*)a.alloc >> 32);
 }
 
-inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 // Runs the collapse from the root, one launch per level, without waiting for
 // the host between levels: launches past the last level find no nodes and
@@ -1305,7 +1740,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     const int boundBlocks = std::min(1024, div_up(n, 256));
     const int nodeCapacity = std::max(1, nInternal);
     const bool group = PRT_WIDE_DP && sahGrouping && nInternal > 0;
-    const bool rebuild = PRT_SAH_REBUILD && sahGrouping && nInternal > 0;
+    const bool rebuild = PRT_SAH_BUILD && sahGrouping && nInternal > 0;
     int device = 0, numSMs = 148;
     if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device);
 
@@ -1313,7 +1748,8 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     float *triBox, *partial, *cbounds, *box;
     uint32_t *keysA, *keysB, *valsA, *valsB, *hist;
     int2 *child, *range;
-    int *parent, *flag, *collapseErr, *marks, *binRef, *sahRoots, *sahSlots, *sahCount;
+    int *parent, *flag, *collapseErr, *marks, *binRef;
+    TopBuffers top{};
     unsigned long long* collapseAlloc;
     float4* dpCost;
     uint2* dpDec;
@@ -1333,9 +1769,20 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         flag = c.take<int>(nodeCapacity);
         box = c.take<float>(6 * (size_t)(2 * n));
         binRef = c.take<int>(nodeCapacity);
-        sahRoots = rebuild ? c.take<int>(nodeCapacity) : nullptr;
-        sahSlots = rebuild ? c.take<int>(n) : nullptr;
-        sahCount = rebuild ? c.take<int>((size_t)n + 1) : nullptr;
+        if (rebuild)
+        {
+            top.maxTasks = n / (kSahLeaves + 1) + 2;
+            top.maxChunks = n / kTopChunk + top.maxTasks + 2;
+            top.task[0] = c.take<TopTask>(top.maxTasks);
+            top.task[1] = c.take<TopTask>(top.maxTasks);
+            top.splits = c.take<TopSplit>(top.maxTasks);
+            top.bins = c.take<uint32_t>((size_t)top.maxTasks * 3 * kTopBins * kBinWords);
+            top.leftCount = c.take<uint32_t>(top.maxChunks);
+            top.scanSums = c.take<uint32_t>(scan_sums_entries(top.maxChunks));
+            top.small = c.take<int>((size_t)n / 2 + 1);
+            top.counters = c.take<int>(3);
+            top.chunks = c.take<int4>(top.maxChunks);
+        }
         collapseAlloc = c.take<unsigned long long>(1);
         collapseErr = c.take<int>(1);
         marks = c.take<int>(kCollapseLevels + 2);
@@ -1377,20 +1824,16 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     radix_sort_pairs(keysA, valsA, keysB, valsB, hist, n, 30, stream);
     if (nInternal > 0)
     {
-        k_karras<<<div_up(nInternal, 256), 256, 0, stream>>>(keysA, n, child, range, parent);
-        BUILD_CHECK(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)nInternal, stream));
         if (rebuild)
         {
-            // sahCount[0..n): slots per subtree start, sahCount[n]: roots
-            BUILD_CHECK(cudaMemsetAsync(sahCount, 0, sizeof(int) * ((size_t)n + 1), stream));
-            k_sah_roots<<<div_up(nInternal, 256), 256, 0, stream>>>(n, range, parent, sahRoots, sahCount + n);
-            k_sah_slots<<<div_up(nInternal, 256), 256, 0, stream>>>(n, range, parent, sahSlots, sahCount);
-            int perSM = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_sah_rebuild, kSahLeaves, 0);
-            k_sah_rebuild<<<std::max(1, perSM) * numSMs, kSahLeaves, 0, stream>>>(n, sahRoots, sahCount + n, triBox,
-                                                                               valsA, child, range, parent, sahSlots);
-            BUILD_CHECK(cudaGetLastError());
+            top.tmp = keysB;   // free after the sort
+            BUILD_CHECK(sah_top_down(n, triBox, cbounds, valsA, child, range, parent, top, numSMs, stream));
         }
+        else
+        {
+            k_karras<<<div_up(nInternal, 256), 256, 0, stream>>>(keysA, n, child, range, parent);
+        }
+        BUILD_CHECK(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)nInternal, stream));
     }
     else
     {

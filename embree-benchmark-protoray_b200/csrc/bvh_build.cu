@@ -559,6 +559,7 @@ struct TopSplit
     int bin;        // left: bins 0..bin
     int nl;         // triangles going left
     int pad;
+    float cmin[2][3], cmax[2][3];   // centroid bounds of the two halves
 };
 
 __device__ __forceinline__ uint32_t ford(float f)
@@ -683,76 +684,150 @@ __global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks
     }
 }
 
-// One thread per task: the least-cost split over the bins of the three axes.
+__device__ __forceinline__ float shfl_ud(float v, int off, bool down)
+{
+    return down ? __shfl_down_sync(0xffffffffu, v, off) : __shfl_up_sync(0xffffffffu, v, off);
+}
+
+// One warp per task, lane b = bin b: the least-cost split over the bins of
+// the three axes (prefix and suffix boxes by warp scans; ties to the lower
+// axis, then the lower bin), and the centroid bounds of the two halves.
 __global__ void k_top_split(const TopTask* __restrict__ tasks, int numTasks, const uint32_t* __restrict__ bins,
                             TopSplit* splits)
 {
-    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ti >= numTasks) return;
+    static_assert(kTopBins == 32, "one lane per bin");
+    const int ti = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (ti >= numTasks) return;   // warp-uniform
+    const int lane = threadIdx.x & 31;
     const TopTask tk = tasks[ti];
     const uint32_t* g = bins + (size_t)ti * 3 * kTopBins * kBinWords;
-    float best = FLT_MAX;
-    TopSplit sp{-1, 0, (tk.hi - tk.lo + 1) / 2, 0};
+    unsigned long long best = ~0ull;   // (cost bits << 32) | (axis * 32 + bin)
     for (int ax = 0; ax < 3; ++ax)
     {
-        float rArea[kTopBins];
-        int rCnt[kTopBins];
-        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-        int cnt = 0;
-        for (int b = kTopBins - 1; b >= 0; --b)
-        {
-            const uint32_t* w = g + (ax * kTopBins + b) * kBinWords;
-            if (w[0])
-                for (int k = 0; k < 3; ++k)
-                {
-                    lo[k] = fminf(lo[k], funord(w[1 + k]));
-                    hi[k] = fmaxf(hi[k], funord(w[4 + k]));
-                }
-            cnt += (int)w[0];
-            rCnt[b] = cnt;
-            rArea[b] = cnt ? box_half_area_lh(lo, hi) : 0.f;
-        }
+        const uint32_t* w = g + (ax * kTopBins + lane) * kBinWords;
+        const int cnt = (int)w[0];
+        float lo[3], hi[3];
+#pragma unroll
         for (int k = 0; k < 3; ++k)
         {
-            lo[k] = FLT_MAX;
-            hi[k] = -FLT_MAX;
+            lo[k] = cnt ? funord(w[1 + k]) : FLT_MAX;
+            hi[k] = cnt ? funord(w[4 + k]) : -FLT_MAX;
         }
-        cnt = 0;
-        for (int b = 0; b < kTopBins - 1; ++b)
+        // left: inclusive prefix over bins 0..lane; right: suffix over lane..31
+        int lc = cnt, rc = cnt;
+        float llo[3], lhi[3], rlo[3], rhi[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
         {
-            const uint32_t* w = g + (ax * kTopBins + b) * kBinWords;
-            if (w[0])
+            llo[k] = rlo[k] = lo[k];
+            lhi[k] = rhi[k] = hi[k];
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const int ulc = __shfl_up_sync(0xffffffffu, lc, off);
+            const int drc = __shfl_down_sync(0xffffffffu, rc, off);
+            float ul[3], uh[3], dl[3], dh[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                ul[k] = shfl_ud(llo[k], off, false);
+                uh[k] = shfl_ud(lhi[k], off, false);
+                dl[k] = shfl_ud(rlo[k], off, true);
+                dh[k] = shfl_ud(rhi[k], off, true);
+            }
+            if (lane >= off)
+            {
+                lc += ulc;
+#pragma unroll
                 for (int k = 0; k < 3; ++k)
                 {
-                    lo[k] = fminf(lo[k], funord(w[1 + k]));
-                    hi[k] = fmaxf(hi[k], funord(w[4 + k]));
+                    llo[k] = fminf(llo[k], ul[k]);
+                    lhi[k] = fmaxf(lhi[k], uh[k]);
                 }
-            cnt += (int)w[0];
-            if (cnt == 0 || rCnt[b + 1] == 0) continue;
-            const float c = box_half_area_lh(lo, hi) * (float)cnt + rArea[b + 1] * (float)rCnt[b + 1];
-            if (c < best)
+            }
+            if (lane + off < 32)
             {
-                best = c;
-                sp.axis = ax;
-                sp.bin = b;
-                sp.nl = cnt;
+                rc += drc;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    rlo[k] = fminf(rlo[k], dl[k]);
+                    rhi[k] = fmaxf(rhi[k], dh[k]);
+                }
             }
         }
+        // split after bin `lane`: the suffix from lane + 1
+        const int nrc = __shfl_down_sync(0xffffffffu, rc, 1);
+        float nlo[3], nhi[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            nlo[k] = __shfl_down_sync(0xffffffffu, rlo[k], 1);
+            nhi[k] = __shfl_down_sync(0xffffffffu, rhi[k], 1);
+        }
+        if (lane < 31 && lc > 0 && nrc > 0)
+        {
+            const float c = box_half_area_lh(llo, lhi) * (float)lc + box_half_area_lh(nlo, nhi) * (float)nrc;
+            const unsigned long long key = ((unsigned long long)__float_as_uint(fmaxf(c, 0.f)) << 32) |
+                                           (unsigned)(ax * kTopBins + lane);
+            best = key < best ? key : best;
+        }
     }
-    splits[ti] = sp;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, best, off);
+        best = o < best ? o : best;
+    }
+    TopSplit sp;
+    sp.pad = 0;
+    if (best == ~0ull)
+    {
+        sp.axis = -1;
+        sp.bin = 0;
+        sp.nl = (tk.hi - tk.lo + 1) / 2;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                sp.cmin[h][k] = tk.cmin[k];
+                sp.cmax[h][k] = tk.cmax[k];
+            }
+    }
+    else
+    {
+        const int code = (int)(best & 0xffffffffu);
+        sp.axis = code / kTopBins;
+        sp.bin = code % kTopBins;
+        const uint32_t* w = g + (sp.axis * kTopBins + lane) * kBinWords;
+        const int cnt = (int)w[0];
+        const bool left = lane <= sp.bin;
+        sp.nl = __reduce_add_sync(0xffffffffu, left ? cnt : 0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            const uint32_t cl = cnt ? w[7 + k] : 0xffffffffu, chh = cnt ? w[10 + k] : 0u;
+            sp.cmin[0][k] = funord(__reduce_min_sync(0xffffffffu, left ? cl : 0xffffffffu));
+            sp.cmax[0][k] = funord(__reduce_max_sync(0xffffffffu, left ? chh : 0u));
+            sp.cmin[1][k] = funord(__reduce_min_sync(0xffffffffu, left ? 0xffffffffu : cl));
+            sp.cmax[1][k] = funord(__reduce_max_sync(0xffffffffu, left ? 0u : chh));
+        }
+    }
+    if (lane == 0) splits[ti] = sp;
 }
 
 // One thread per task: the two halves become internal nodes (next-level tasks
 // or rebuild subtrees) or leaves.
 __global__ void k_top_children(const TopTask* __restrict__ tasks, int numTasks, const TopSplit* __restrict__ splits,
-                               const uint32_t* __restrict__ bins, int n, TopTask* nextTasks, int* numNext,
+                               int n, TopTask* nextTasks, int* numNext,
                                int* small, int* numSmall, int* nodeCounter, int2* child, int2* range, int* parent)
 {
     const int ti = blockIdx.x * blockDim.x + threadIdx.x;
     if (ti >= numTasks) return;
     const TopTask tk = tasks[ti];
     const TopSplit sp = splits[ti];
-    const uint32_t* g = bins + (size_t)ti * 3 * kTopBins * kBinWords;
     const int lo[2] = {tk.lo, tk.lo + sp.nl}, hi[2] = {tk.lo + sp.nl - 1, tk.hi};
     int refs[2];
     for (int side = 0; side < 2; ++side)
@@ -778,32 +853,10 @@ __global__ void k_top_children(const TopTask* __restrict__ tasks, int numTasks, 
         c.hi = hi[side];
         c.node = id;
         c.pad = 0;
-        if (sp.axis < 0)
+        for (int k = 0; k < 3; ++k)
         {
-            for (int k = 0; k < 3; ++k)
-            {
-                c.cmin[k] = tk.cmin[k];
-                c.cmax[k] = tk.cmax[k];
-            }
-        }
-        else
-        {
-            for (int k = 0; k < 3; ++k)
-            {
-                c.cmin[k] = FLT_MAX;
-                c.cmax[k] = -FLT_MAX;
-            }
-            const int b0 = side == 0 ? 0 : sp.bin + 1, b1 = side == 0 ? sp.bin : kTopBins - 1;
-            for (int b = b0; b <= b1; ++b)
-            {
-                const uint32_t* w = g + (sp.axis * kTopBins + b) * kBinWords;
-                if (!w[0]) continue;
-                for (int k = 0; k < 3; ++k)
-                {
-                    c.cmin[k] = fminf(c.cmin[k], funord(w[7 + k]));
-                    c.cmax[k] = fmaxf(c.cmax[k], funord(w[10 + k]));
-                }
-            }
+            c.cmin[k] = sp.cmin[side][k];
+            c.cmax[k] = sp.cmax[side][k];
         }
         nextTasks[atomicAdd(numNext, 1)] = c;
     }
@@ -983,10 +1036,10 @@ cudaError_t sah_top_down(int n, const float* triBox, const float* cbounds, uint3
         const int words = numTasks * 3 * kTopBins * kBinWords;
         k_top_init_bins<<<std::min(div_up(words, 256), 4 * numSMs), 256, 0, stream>>>(B.bins, words);
         k_top_bin<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], perm, triBox, B.bins);
-        k_top_split<<<div_up(numTasks, 128), 128, 0, stream>>>(B.task[cur], numTasks, B.bins, B.splits);
+        k_top_split<<<div_up(numTasks, 4), 128, 0, stream>>>(B.task[cur], numTasks, B.bins, B.splits);
         e = cudaMemsetAsync(B.counters, 0, sizeof(int), stream);
         if (e != cudaSuccess) break;
-        k_top_children<<<div_up(numTasks, 128), 128, 0, stream>>>(B.task[cur], numTasks, B.splits, B.bins, n,
+        k_top_children<<<div_up(numTasks, 128), 128, 0, stream>>>(B.task[cur], numTasks, B.splits, n,
                                                                    B.task[cur ^ 1], B.counters, B.small,
                                                                    B.counters + 1, B.counters + 2, child, range,
                                                                    parent);

@@ -1,4 +1,4 @@
-// GPU LBVH build into the compressed 8-wide node layout of prt_device.cuh.
+// GPU BVH build into the compressed 8-wide node layout of prt_device.cuh.
 //
 // Replaces the acceleration-structure build of the reference's GPU path
 // (OptiX Prime model->setTriangles/update, accel/optix/optix_intersector_stream_cuda.cpp:49-59;
@@ -8,11 +8,14 @@
 //   1. triangle boxes + centroid bounds (block partials, one final reduce)
 //   2. 30-bit Morton codes of the centroids (10 bits per axis)
 //   3. stable LSD radix sort of (code, triangle) pairs, 8-bit digits
-//   4. binary radix tree over the sorted codes (Karras, HPG 2012); equal
-//      codes are ordered by their position, so duplicates are handled
+//   4. the binary tree: for the high-quality build (default) a full SAH tree
+//      built top-down from that order (binned SAH above kSahLeaves triangles,
+//      an exact sweep SAH per block below); otherwise the binary radix tree
+//      over the sorted codes (Karras, HPG 2012; equal codes are ordered by
+//      their position, so duplicates are handled)
 //   5. bottom-up bounds refit (second child to arrive computes the union),
 //      fused with the SAH-optimal grouping of the binary nodes into 8-wide
-//      nodes (dynamic program of Ylitie et al. 2017 over the LBVH)
+//      nodes (dynamic program of Ylitie et al. 2017 over the binary tree)
 //   6. top-down collapse into 8-wide nodes, one tree level per launch (no
 //      host round trip between levels), one 8-lane group per node:
 //      children are the roots chosen by the dynamic program (or, for trees
@@ -1068,7 +1071,7 @@ cudaError_t sah_top_down(int n, const float* triBox, const float* cbounds, uint3
 //
 // The node box is the union of the children's boxes.  With kGroup the same
 // pass runs the dynamic program of Ylitie, Karras and Laine (HPG 2017,
-// sec. 4.1) over the LBVH: C(u, i), i = 1..8, is the least SAH cost of
+// sec. 4.1) over the binary tree: C(u, i), i = 1..8, is the least SAH cost of
 // representing subtree u by at most i roots (children of the enclosing 8-wide
 // node).  A leaf root costs area x cTri x triangles, an 8-wide node area x
 // cNode plus the best split of its 8 slots between the binary children;

@@ -545,7 +545,8 @@ __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __
 // the range in shared memory, then merged with atomics), its triangles are
 // partitioned into the two halves of the range, and the halves become the
 // next level's tasks, k_sah_rebuild's subtrees (2..kSahLeaves triangles) or
-// leaves.  One host read-back per level sizes the next level's launches.
+// leaves.  One host read-back per level (the next tasks' count and ranges)
+// sizes the next level's launches.
 constexpr int kTopBins = 32;
 constexpr int kTopChunk = 4096;        // triangles per block of the binning and partition passes
 constexpr int kBinWords = 13;          // count, box lo/hi, centroid lo/hi (order-preserving float bits)
@@ -1016,15 +1017,13 @@ cudaError_t sah_top_down(int n, const float* triBox, const float* cbounds, uint3
     cudaError_t e = cudaGetLastError();
     int numTasks = n > kSahLeaves ? 1 : 0;
     int cur = 0;
-    std::vector<TopTask> host;
+    std::vector<TopTask> host(1);   // the tasks' ranges (the root's is known)
+    host[0].lo = 0;
+    host[0].hi = n - 1;
     std::vector<int4> chunks;
     while (e == cudaSuccess && numTasks > 0)
     {
         if (numTasks > B.maxTasks) return cudaErrorInvalidValue;
-        host.resize(numTasks);
-        e = cudaMemcpyAsync(host.data(), B.task[cur], sizeof(TopTask) * numTasks, cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) break;
         chunks.clear();
         for (int ti = 0; ti < numTasks; ++ti)
         {
@@ -1051,7 +1050,13 @@ cudaError_t sah_top_down(int n, const float* triBox, const float* cbounds, uint3
         k_top_partition<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], B.splits, perm, triBox, B.leftCount, B.tmp);
         k_top_copy<<<nch, 256, 0, stream>>>(B.chunks, B.tmp, perm);
         e = cudaGetLastError();
+        // one read-back per level: the count and the ranges of the next tasks
+        // (at most two per task)
+        const int cap = std::min(B.maxTasks, 2 * numTasks);
+        host.resize(cap);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&numTasks, B.counters, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host.data(), B.task[cur ^ 1], sizeof(TopTask) * cap, cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         cur ^= 1;
     }

@@ -538,9 +538,10 @@ __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __
 
 // --- 4c. top-down binned SAH above kSahLeaves triangles ------------------------
 //
-// The high-quality build does not use the Morton hierarchy's top either: from
-// the root, every task (a node and its contiguous range of triangles) with
-// more than kSahLeaves triangles is split by the least SAH cost over
+// The high-quality build makes a full SAH tree instead of the Morton
+// hierarchy.  From the root (the triangles in Morton order), every task (a
+// node and its contiguous range of triangles) with more than kSahLeaves
+// triangles is split by the least SAH cost over
 // kTopBins centroid bins per axis (bin boxes and counts gathered per chunk of
 // the range in shared memory, then merged with atomics), its triangles are
 // partitioned into the two halves of the range, and the halves become the

@@ -303,7 +303,8 @@ class Context:
         self._check(self.L.prt_set_leaf_size(self.h, n), "prt_set_leaf_size")
 
     def set_build_quality(self, high: bool):
-        """True: SAH grouping into 8-wide nodes (default); False: greedy."""
+        """True: full SAH tree with SAH grouping into 8-wide nodes (default);
+        False: Morton LBVH with greedy grouping (faster to build)."""
         self._check(self.L.prt_set_build_quality(self.h, 1 if high else 0), "prt_set_build_quality")
 
     def build(self) -> Dict[str, float]:

@@ -150,9 +150,10 @@ int prt_build_accel(prt_ctx* ctx, prt_build_stats* stats);
 int prt_set_leaf_size(prt_ctx* ctx, int maxTrianglesPerLeaf);
 /* Build quality for the next build, the reference's high-quality switch
  * (`-no-sbvh` turns it off, accel/embree/embree_intersector.cpp:24,56-57):
- * high (1, the default) groups the LBVH into 8-wide nodes by the SAH dynamic
- * program; low (0) opens the largest child greedily, which is faster to build
- * and gives a tree of more, emptier nodes. */
+ * high (1, the default) builds a full SAH binary tree and groups it into
+ * 8-wide nodes by the SAH dynamic program; low (0) builds the Morton LBVH and
+ * opens the largest child greedily, which is several times faster to build
+ * and traces slower (more, emptier nodes over a lower-quality tree). */
 int prt_set_build_quality(prt_ctx* ctx, int high);
 
 /* --- camera (DeviceCuda::initCamera, render/device_cuda.cpp:175-200) --- */

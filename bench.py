@@ -431,7 +431,7 @@ def run_kernel_tour(prt, torch, device):
     """Launches every kernel family of the library once on a case whose inputs
     exceed L2 where the kernel reads bulk data, for profiler captures
     (`ncu ... python bench.py --kernel-tour`); prints one JSON line of
-    CUDA-event times.  Phases: LBVH build of 2000 level-4 icospheres (10.2M
+    CUDA-event times.  Phases: BVH build of 2000 level-4 icospheres (10.2M
     triangles); 4M incoherent closest-hit and any-hit queries on the terrain;
     one diffuse2 render (960x540, 4 spp); path-replay forward and backward
     (small scene, 512x512, 4 spp, per-triangle albedo); a batch of 8 requests;

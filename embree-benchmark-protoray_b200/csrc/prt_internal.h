@@ -120,6 +120,29 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
                std::string& err, BuildInfo* info, int leafMax, bool sahGrouping = true,
                DeviceScratch* scratch = nullptr);
 
+// Full SAH binary tree for the high-quality build (sah_build.cu): scratch
+// carved by sah_tree_carve (tmp: n free words the caller supplies), then
+// sah_build_tree writes child / range / parent of the n - 1 internal nodes
+// (root 0, leaves ~p for position p of perm) and reorders perm.
+struct TopTask;
+struct TopSplit;
+struct SahTreeBuffers
+{
+    TopTask* task[2];
+    TopSplit* splits;
+    uint32_t* bins;
+    uint32_t* leftCount;   // per chunk, then its exclusive scan
+    uint32_t* scanSums;
+    int* small;
+    int* counters;
+    int4* chunks;
+    uint32_t* tmp;
+    int maxTasks, maxChunks;
+};
+void sah_tree_carve(Carve& c, int n, SahTreeBuffers& B);
+cudaError_t sah_build_tree(int n, const float* triBox, const float* cbounds, uint32_t* perm, int2* child, int2* range,
+                           int* parent, const SahTreeBuffers& B, int numSMs, cudaStream_t stream);
+
 // Sort and scan primitives (sort_scan.cu).  radix_sort_pairs sorts (key, value)
 // pairs stably on key bits [0, bits); the sorted pairs end in keys/vals (the
 // pointers are swapped with the temporaries as needed).  hist needs

@@ -35,6 +35,10 @@ WORKLOAD = ("terrain: 1024x512-quad heightfield + 256 level-3 icospheres, 1,376,
             "1920x1080, 64 spp, maxDepth 5")
 UNIT = "Mrays/s"
 W, H, SPP, DEPTH = 1920, 1080, 64, 5
+# the 10M-triangle stress configuration, reported beside the headline
+C2_WORKLOAD = ("spheres10m: 2000 level-4 icospheres, log-uniform radius 0.1-5 in a 200^3 box, 10,240,000 tris; "
+               "camera on the box's front face; 1920x1080, 16 spp, maxDepth 8")
+C2_W, C2_H, C2_SPP, C2_DEPTH = 1920, 1080, 16, 8
 ALGO_BYTES_PER_RAY = 192   # compulsory wavefront record traffic per ray of the separate-kernel reference design
 L2_BYTES = 126 * 1024 * 1024
 
@@ -177,43 +181,57 @@ def c_stdout_to_stderr():
         os.close(saved)
 
 
-def cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None):
+def cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, scene="terrain"):
     with c_stdout_to_stderr():
-        return _cpu_reference_run(steps, warmup, frames_per_step, sample_seconds)
+        return _cpu_reference_run(steps, warmup, frames_per_step, sample_seconds, scene)
 
 
-def _cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None):
+def _cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, scene="terrain"):
     """Times the reference's own diffuseStream renderer (oracle/_ref) on the
-    host cores at 1920x1080, maxDepth 5; one step = `frames_per_step` frames."""
+    host cores; one step = `frames_per_step` 1-spp frames.  scene "terrain":
+    1920x1080, maxDepth 5; "spheres10m": the 10.24M-triangle icosphere field
+    from its in-field camera, 1920x1080, maxDepth 8."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     import scenes
     if not oracle.Reference.available():
         return None
-    mesh, view = scenes.terrain_scene()
+    if scene == "terrain":
+        mesh, view = scenes.terrain_scene()
+        w, h, depth = W, H, DEPTH
+    else:
+        mesh, _ = scenes.spheres10m_scene()
+        view = scenes.field_view(mesh)
+        w, h, depth = C2_W, C2_H, C2_DEPTH
     import tempfile
     d = tempfile.mkdtemp(prefix="prt_bench_")
-    path = scenes.write_scene(d, "terrain", mesh, view)
+    path = scenes.write_scene(d, scene, mesh, view)
     R = oracle.Reference()
     rs = R.open(path)
+    tb = time.perf_counter()
     rs.build(1)
+    build_s = time.perf_counter() - tb
     cores = int(os.environ.get("PRT_REF_THREADS", "0")) or (os.cpu_count() or 1)
     for _ in range(warmup):
-        rs.render("diffuseStream", view, W, H, frames_per_step, DEPTH, accel=1, want_sums=False)
+        rs.render("diffuseStream", view, w, h, frames_per_step, depth, accel=1, want_sums=False)
     rays = 0.0
     secs = 0.0
     t0 = time.perf_counter()
     n = 0
     while n < steps:
-        _, st = rs.render("diffuseStream", view, W, H, frames_per_step, DEPTH, accel=1, want_sums=False)
+        _, st = rs.render("diffuseStream", view, w, h, frames_per_step, depth, accel=1, want_sums=False)
         rays += st["rays"]
         secs += st["seconds"]
         n += 1
         if sample_seconds and time.perf_counter() - t0 > sample_seconds:
             break
     wall = time.perf_counter() - t0
+    try:
+        os.remove(path)
+    except OSError:
+        pass
     return {"value": rays / 1e6 / secs, "rays": rays, "seconds": secs, "wall": wall, "frames": n * frames_per_step,
-            "cores": cores, "cpu": cpu_model()}
+            "cores": cores, "cpu": cpu_model(), "build_s": build_s}
 
 
 def cpu_model():
@@ -366,6 +384,66 @@ def run_fwd_bwd(prt, torch, device):
     f, b = min(fw), min(fb)
     return {"fwd_ms": round(f, 3), "fwd_bwd_ms": round(b, 3), "ratio": round(b / f, 3),
             "config": "small scene 82K tris, 512x512, 16 spp, maxDepth 5, per-triangle albedo"}
+
+
+def run_c2(prt, torch, device, steps, warmup, cpu_seconds):
+    """The 10.24M-triangle icosphere field at 1920x1080, 16 spp, maxDepth 8:
+    build time of a context's first BVH build and of a rebuild, device and
+    end-to-end Mrays/s (L2 flushed between timed steps), and the reference's
+    diffuseStream on the host cores on the same scene and camera."""
+    import scenes
+    mesh, _ = scenes.spheres10m_scene()
+    view = scenes.field_view(mesh)
+    c = prt.Context(device)
+    c.load_mesh(mesh.indices, mesh.positions)
+    b0 = c.build()
+    b1 = c.build()
+    c.init_frame(C2_W, C2_H)
+    cam = prt.camera_from_view(view, C2_W, C2_H)
+    c.set_camera(cam)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
+    for _ in range(warmup):
+        c.set_pass(0)
+        c.render(C2_SPP, C2_DEPTH, accumulate=False)
+    rays, ms = 0, 0.0
+    for s in range(steps):
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        c.set_pass(0)
+        st = c.render(C2_SPP, C2_DEPTH, accumulate=False)
+        rays += st["ray"]
+        ms += st["ms"]
+    host_img = torch.empty((C2_H, C2_W, 4), dtype=torch.float32).pin_memory()
+    torch.cuda.synchronize()
+    e_rays = 0
+    t0 = time.perf_counter()
+    for s in range(steps):
+        c.set_camera(cam)
+        c.set_pass(0)
+        st = c.render(C2_SPP, C2_DEPTH, accumulate=False)
+        c.read_accum(host_img)
+        e_rays += st["ray"]
+    torch.cuda.synchronize()
+    e_secs = time.perf_counter() - t0
+    c.close()
+    out = {"workload": C2_WORKLOAD, "triangles": mesh.tri_count, "width": C2_W, "height": C2_H, "spp": C2_SPP,
+           "maxDepth": C2_DEPTH, "steps": steps, "value": round(rays / 1e6 / (ms / 1e3), 2), "unit": UNIT,
+           "ms_per_step": round(ms / steps, 3), "rays_per_step": int(rays / steps),
+           "e2e": {"value": round(e_rays / 1e6 / e_secs, 2), "unit": UNIT, "h2d_bytes_per_step": 76,
+                   "d2h_bytes_per_step": C2_W * C2_H * 16},
+           "buildMs_first": round(b0["buildMs"], 2), "buildMs": round(b1["buildMs"], 2),
+           "buildMprim": round(mesh.tri_count / 1e3 / b1["buildMs"], 2), "bvh8_nodes": b1["nodeCount"],
+           "bvh8_levels": b1["levels"]}
+    if cpu_seconds > 0:
+        r = cpu_reference_run(1000, 1, sample_seconds=cpu_seconds, scene="spheres10m")
+        if r is not None:
+            out["cpu_baseline"] = {
+                "value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                "build_s": round(r["build_s"], 2),
+                "sample": (f"reference diffuseStream renderer + project CPU BVH (Embree 3 absent), same scene and "
+                           f"camera, {r['frames']} frames x 1 spp, maxDepth {C2_DEPTH}, {r['wall']:.1f} s")}
+            out["vs_cpu"] = round(out["value"] / r["value"], 1)
+    return out
 
 
 def run_mesh_build(prt, torch, device):
@@ -522,9 +600,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--no-extras", action="store_true", help="skip the batched and fwd+bwd measurements")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched, fwd+bwd, mesh-build and 10M-triangle measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch configuration")
     ap.add_argument("--width", type=int, default=W, help="smaller frames are for profiling captures only")
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
@@ -561,6 +641,15 @@ def main():
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
     pass0, npass = rank_pass_range(rank, world, SPP)
+
+    # queue and launch sizes from the library's autotuner, timed on this
+    # workload before the warm-up
+    tune = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        tune = ctx.autotune(npass, DEPTH)
+        tune = {"block": tune["blockSize"], "blocksPerSM": tune["blocksPerSM"], "pathsPerWave": tune["pathsPerWave"],
+                "chains": tune["concurrentWaves"], "tuning_s": round(time.perf_counter() - t0, 2)}
 
     def step(pass_base):
         ctx.set_pass(pass_base)
@@ -644,6 +733,8 @@ def main():
         extras["batched"] = run_batch(prt, torch, local)
         extras["differentiable"] = run_fwd_bwd(prt, torch, local)
         extras["mesh_build"] = run_mesh_build(prt, torch, local)
+        extras["c2"] = run_c2(prt, torch, local, args.steps, args.warmup,
+                              0 if (args.no_cpu or world > 1) else args.cpu_seconds / 2)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -659,7 +750,8 @@ def main():
                        "maxDepth": DEPTH, "triangles": mesh.tri_count, "l2": "flushed between timed steps",
                        "parallelism": f"replicas{world}", "buildMs": round(build["buildMs"], 2),
                        "buildMprim": round(build["buildMprim"], 2), "bvh8_nodes": build["nodeCount"],
-                       "bvh8_levels": build["levels"]},
+                       "bvh8_levels": build["levels"],
+                       "launch_config": tune or {"autotune": "off", **ctx.get_tune()}},
             "rays_per_step": int(rays / args.steps),
             "wall_s": round(wall, 3),
             "e2e": {"value": round(e_value, 2), "unit": UNIT, "h2d_bytes_per_step": 76,

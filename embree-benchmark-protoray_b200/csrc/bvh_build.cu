@@ -918,8 +918,16 @@ int collapse_levels(const CollapseArgs& a, int n, int numSMs, cudaStream_t strea
         }                                                                                                      \
     } while (0)
 
-int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
-               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping, DeviceScratch* scratch)
+namespace {
+
+constexpr const char* kTooDeep = "BVH8 is deeper than the traversal stack";
+
+// sahTree: the top-down SAH binary tree (else the Karras hierarchy over the
+// Morton order); sahGrouping: the SAH-optimal grouping into 8-wide nodes
+// (else greedy).
+int build_bvh8_tree(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
+                    std::string& err, BuildInfo* info, int leafMax, bool sahTree, bool sahGrouping,
+                    DeviceScratch* scratch)
 {
     (void)nv;
     int status = PRT_OK;
@@ -932,7 +940,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
     const int boundBlocks = std::min(1024, div_up(n, 256));
     const int nodeCapacity = std::max(1, nInternal);
     const bool group = PRT_WIDE_DP && sahGrouping && nInternal > 0;
-    const bool rebuild = sahGrouping && nInternal > 0;   // the SAH tree (sah_build.cu)
+    const bool rebuild = sahTree && nInternal > 0;   // the SAH tree (sah_build.cu)
     int device = 0, numSMs = 148;
     if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device);
 
@@ -1076,7 +1084,7 @@ int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& o
         out.levels = levels;
         if (2 * levels > kStackMax)
         {
-            err = "BVH8 is deeper than the traversal stack";
+            err = kTooDeep;
             status = PRT_EINTERNAL;
             goto done;
         }
@@ -1104,6 +1112,25 @@ done:
     if (ev1) cudaEventDestroy(ev1);
     if (status != PRT_OK) out.release();
     return status;
+}
+
+} // namespace
+
+int build_bvh8(const float* dPos, int nv, const int* dIdx, int nt, Bvh8Device& out, cudaStream_t stream,
+               std::string& err, BuildInfo* info, int leafMax, bool sahGrouping, DeviceScratch* scratch)
+{
+    int st = build_bvh8_tree(dPos, nv, dIdx, nt, out, stream, err, info, leafMax, sahGrouping, sahGrouping, scratch);
+    if (st == PRT_EINTERNAL && sahGrouping && err == kTooDeep)
+    {
+        // The SAH tree has no depth limit: a chain-shaped input (triangle sizes
+        // shrinking geometrically, each split peeling one off) can come out
+        // deeper than the traversal stack even after greedy grouping.  The
+        // Karras hierarchy over 30-bit Morton codes is at most about 30 + log2(n)
+        // binary levels deep, so build that instead.
+        err.clear();
+        st = build_bvh8_tree(dPos, nv, dIdx, nt, out, stream, err, info, leafMax, false, true, scratch);
+    }
+    return st;
 }
 
 } // namespace prt_b200

@@ -15,15 +15,21 @@
 //   * the frame may hold at most kNoAllocMaxPaths pixels after rounding up to
 //     8x8 tiles (524288, e.g. 1024x512 or 960x544); larger frames are
 //     rejected with PRT_EINVAL;
-//   * g_scratch occupies 36 MiB on every GPU that loads the library, until the
+//   * g_scratch occupies 40 MiB on every GPU that loads the library, until the
 //     process exits;
 //   * all calls on a device share g_scratch, which keeps the last call's
 //     contents: each call clears the counters it needs before using them, and
 //     calls that overlap on the GPU (concurrent streams or host threads) race
 //     on the shared queues — serialise them;
-//   * the first call on a device looks up the array's device address (with
-//     that device current) and caches it; make that first call before any
-//     stream capture on the calling thread.
+//   * the first call in a CUDA context of a device looks up the array's device
+//     address in that context (with that device current) and caches it; make
+//     that first call before any stream capture on the calling thread.  A
+//     later context on the same device (after cudaDeviceReset, for example)
+//     is recognised by its context id and looked up again;
+//   * the caller's current device is restored before the call returns.
+#include <cuda.h>
+
+#include <cstdint>
 #include <mutex>
 
 #include "prt_internal.h"
@@ -38,7 +44,8 @@ constexpr int kNoAllocCounters = 64 + 2;   // one slot per bounce depth (max dep
 struct NoAllocScratch
 {
     PathRec queue[2][kNoAllocMaxPaths];
-    float thr[2][kNoAllocMaxPaths];
+    float thr[2][kNoAllocMaxPaths];   // per-path throughput (per-triangle albedo)
+    float L[2][kNoAllocMaxPaths];     // radiance gathered so far (next-event estimation)
     int counts[kNoAllocCounters];
     int fetch[kNoAllocCounters];
     unsigned long long rays;
@@ -48,29 +55,103 @@ struct NoAllocScratch
 static __device__ __align__(256) NoAllocScratch g_scratch;
 
 constexpr int kMaxDevices = 64;
-std::mutex g_lock;
-NoAllocScratch* g_addr[kMaxDevices] = {};
 
-// Device address of g_scratch on `device` (which is current); resolved once.
+struct AddressCache
+{
+    unsigned long long ctxId = 0;   // CUDA context the address belongs to (0: none yet)
+    NoAllocScratch* addr = nullptr;
+};
+
+std::mutex g_lock;
+AddressCache g_cache[kMaxDevices];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the CUDA context current on this thread, through the driver entry
+// points the runtime hands out (no link against libcuda needed).
+cudaError_t current_context_id(unsigned long long* id)
+{
+    static CtxGetCurrentFn getCurrent = nullptr;
+    static CtxGetIdFn getId = nullptr;
+    if (!getCurrent || !getId)
+    {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0);
+        if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return e;
+        if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return cudaErrorSymbolNotFound;
+        getCurrent = reinterpret_cast<CtxGetCurrentFn>(f0);
+        getId = reinterpret_cast<CtxGetIdFn>(f1);
+    }
+    CUcontext c = nullptr;
+    if (getCurrent(&c) != CUDA_SUCCESS || !c) return cudaErrorDeviceUninitialized;
+    if (getId(c, id) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
+}
+
+// Device address of g_scratch in the current context of `device` (which is
+// current); looked up once per context.
 cudaError_t scratch_address(int device, NoAllocScratch** out)
 {
+    unsigned long long id = 0;
+    cudaError_t e = current_context_id(&id);
+    if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> guard(g_lock);
-    if (!g_addr[device])
+    AddressCache& c = g_cache[device];
+    if (c.ctxId != id || !c.addr)
     {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess) return e;
-        g_addr[device] = static_cast<NoAllocScratch*>(p);
+        c.addr = static_cast<NoAllocScratch*>(p);
+        c.ctxId = id;
     }
-    *out = g_addr[device];
+    *out = c.addr;
     return cudaSuccess;
+}
+
+// Restores the caller's current device when the call returns.
+struct DeviceRestore
+{
+    int prev = -1;
+    DeviceRestore()
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+        {
+            cudaGetLastError();
+            prev = -1;
+        }
+    }
+    ~DeviceRestore()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// accum must be device (or managed) memory of `device`, 16-byte aligned (the
+// kernels add float4 records to it).
+bool accum_usable(const float* accum, int device)
+{
+    if (reinterpret_cast<uintptr_t>(accum) % 16 != 0) return false;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, accum) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    if (attr.type == cudaMemoryTypeManaged) return true;
+    return attr.type == cudaMemoryTypeDevice && attr.device == device;
 }
 
 } // namespace
 
 // Scene/camera/stream accessors of the context (prt_api.cu).
 int ctx_noalloc_view(prt_ctx* ctx, SceneDev* scene, int* device, cudaStream_t* stream, int* numSMs, LaunchCfg* cfg,
-                     float* sky, bool* albedo);
+                     float* sky, bool* albedo, bool* nee);
 int ctx_fail(prt_ctx* ctx, int status, const char* msg);
 
 } // namespace prt_b200
@@ -86,8 +167,8 @@ extern "C" int prt_render_noalloc(prt_ctx* ctx, const prt_camera* cam, int width
     cudaStream_t stream = nullptr;
     LaunchCfg cfg;
     float sky = 1.0f;
-    bool albedo = false;
-    int st = ctx_noalloc_view(ctx, &scene, &device, &stream, &numSMs, &cfg, &sky, &albedo);
+    bool albedo = false, nee = false;
+    int st = ctx_noalloc_view(ctx, &scene, &device, &stream, &numSMs, &cfg, &sky, &albedo, &nee);
     if (st != PRT_OK) return st;
     if (!cam || !accum || width <= 0 || height <= 0 || pass0 < 0 || spp < 0 || maxDepth < 0 ||
         maxDepth > kNoAllocCounters - 2)
@@ -98,8 +179,12 @@ extern "C" int prt_render_noalloc(prt_ctx* ctx, const prt_camera* cam, int width
         return ctx_fail(ctx, PRT_EINVAL,
                         "prt_render_noalloc: frame too large (at most 524288 pixels after rounding to 8x8 tiles)");
     if (device < 0 || device >= kMaxDevices) return ctx_fail(ctx, PRT_EINVAL, "prt_render_noalloc: device index");
+    DeviceRestore restore;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return ctx_fail(ctx, PRT_ECUDA, cudaGetErrorString(e));
+    if (!accum_usable(accum, device))
+        return ctx_fail(ctx, PRT_EINVAL,
+                        "prt_render_noalloc: accum must be 16-byte aligned device memory of the context's GPU");
     NoAllocScratch* s = nullptr;
     e = scratch_address(device, &s);
     if (e != cudaSuccess) return ctx_fail(ctx, PRT_ECUDA, cudaGetErrorString(e));
@@ -142,6 +227,8 @@ extern "C" int prt_render_noalloc(prt_ctx* ctx, const prt_camera* cam, int width
             a.qout = s->queue[d & 1];
             a.thrIn = albedo && d > 0 ? s->thr[(d - 1) & 1] : nullptr;
             a.thrOut = albedo ? s->thr[d & 1] : nullptr;
+            a.Lin = nee && d > 0 ? s->L[(d - 1) & 1] : nullptr;
+            a.Lout = nee ? s->L[d & 1] : nullptr;
             float t = 1.0f;
             for (int k = 0; k < d; ++k) t *= 0.8f;
             a.thrConst = t;

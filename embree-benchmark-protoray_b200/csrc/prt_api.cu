@@ -1132,6 +1132,20 @@ int prt_intersect(prt_ctx* ctx, const prt_ray* rays, prt_hit* hits, int n, void*
     return PRT_OK;
 }
 
+int prt_primary_rays(prt_ctx* ctx, int pass, prt_ray* rays, void* stream)
+{
+    int st = check_ready(ctx, true);
+    if (st != PRT_OK) return st;
+    if (pass < 0 || !rays) return fail(ctx, PRT_EINVAL, "invalid pass or ray buffer");
+    if (!is_device_ptr(rays)) return fail(ctx, PRT_EINVAL, "prt_primary_rays takes a device pointer");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    ctx->launches += launch_primary_rays(camera_dev(ctx->cam, ctx->W, ctx->H), pass, (RayRec*)rays, s);
+    CK(cudaGetLastError());
+    if (!stream) CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
 int prt_occluded(prt_ctx* ctx, const prt_ray* rays, float* out, int n, void* stream)
 {
     int st = check_ready(ctx, false);
@@ -1399,60 +1413,111 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
 {
     int st = check_ready(ctx, true);
     if (st != PRT_OK) return st;
-    if (spp <= 0) return fail(ctx, PRT_EINVAL, "autotune needs spp > 0");
+    if (spp <= 0 || maxDepth < 0 || maxDepth > kMaxDepthCap)
+        return fail(ctx, PRT_EINVAL, "autotune needs spp > 0 and 0 <= maxDepth <= 64");
     CK(cudaSetDevice(ctx->device));
     const long long perPass = (long long)((ctx->W + 7) / 8) * ((ctx->H + 7) / 8) * 64;
-    LaunchCfg saved = ctx->cfg;
-    LaunchCfg bestCfg = saved;
-    double bestMray = -1;
-    const int blocks[] = {64, 128};
-    const int perSM[] = {0, 2, 4};
-    const long long waves[] = {1, 2, 4};
-    const int chainOpts[] = {1, 2};
-    for (int b : blocks)
-        for (int s : perSM)
-            for (int ch : chainOpts)
-            for (long long wv : waves)
+    const LaunchCfg saved = ctx->cfg;
+
+    // Throughput of one configuration: the best of two timed renders of the
+    // caller's workload after one untimed render (which also records and
+    // instantiates the configuration's graph).
+    auto measure = [&](const LaunchCfg& cfg, double* mray) -> int {
+        ctx->cfg = cfg;
+        clear_graphs(ctx);
+        *mray = 0;
+        for (int rep = 0; rep < 3; ++rep)
+        {
+            prt_render_stats rs;
+            CK(cudaMemsetAsync(ctx->dPass, 0, sizeof(int), ctx->stream));
+            int s2 = prt_render(ctx, spp, maxDepth, 0, &rs);
+            if (s2 != PRT_OK) return s2;
+            if (rep > 0) *mray = std::max(*mray, rs.mray);
+        }
+        return PRT_OK;
+    };
+
+    // Candidate values per parameter.  Wave sizes: the automatic size and 1..16
+    // passes of this frame (at least 64K and at most 64M paths).
+    std::vector<long long> waveOpts = {0};
+    for (long long k : {1, 2, 4, 8, 16})
+    {
+        long long ppw = std::min<long long>(std::max<long long>(perPass * k, 1 << 16), 1LL << 26);
+        if (std::find(waveOpts.begin(), waveOpts.end(), ppw) == waveOpts.end()) waveOpts.push_back(ppw);
+    }
+    const int chainOpts[] = {1, 2, 3, 4};
+    const int perSMOpts[] = {0, 4, 6};
+    const int blockOpts[] = {64, 128};
+
+    // Coordinate descent from the current configuration: one parameter at a
+    // time, a candidate replaces the incumbent only if it is more than 1%
+    // faster (the spread of repeated renders), at most three sweeps.
+    LaunchCfg cur = saved;
+    double curM = 0;
+    st = measure(cur, &curM);
+    for (int sweep = 0; sweep < 3 && st == PRT_OK; ++sweep)
+    {
+        bool improved = false;
+        auto consider = [&](LaunchCfg c) -> int {
+            if (c.block == cur.block && c.blocksPerSM == cur.blocksPerSM && c.pathsPerWave == cur.pathsPerWave &&
+                c.chains == cur.chains)
+                return PRT_OK;
+            double m = 0;
+            int s2 = measure(c, &m);
+            if (s2 == PRT_OK && m > curM * 1.01)
             {
-                long long ppw = std::max<long long>(perPass * wv, 1 << 16);
-                ctx->cfg.block = b;
-                ctx->cfg.blocksPerSM = s;
-                ctx->cfg.pathsPerWave = (int)std::min<long long>(ppw, 1LL << 30);
-                ctx->cfg.chains = ch;
-                prt_render_stats rs;
-                CK(cudaMemsetAsync(ctx->dPass, 0, sizeof(int), ctx->stream));
-                st = prt_render(ctx, spp, maxDepth, 0, &rs);
-                if (st != PRT_OK)
-                {
-                    ctx->cfg = saved;
-                    return st;
-                }
-                // second run: graph already instantiated
-                CK(cudaMemsetAsync(ctx->dPass, 0, sizeof(int), ctx->stream));
-                st = prt_render(ctx, spp, maxDepth, 0, &rs);
-                if (st != PRT_OK)
-                {
-                    ctx->cfg = saved;
-                    return st;
-                }
-                if (rs.mray > bestMray)
-                {
-                    bestMray = rs.mray;
-                    bestCfg = ctx->cfg;
-                }
-                clear_graphs(ctx);
+                cur = c;
+                curM = m;
+                improved = true;
             }
-    ctx->cfg = bestCfg;
+            return s2;
+        };
+        for (long long w : waveOpts)
+        {
+            LaunchCfg c = cur;
+            c.pathsPerWave = (int)w;
+            if ((st = consider(c)) != PRT_OK) break;
+        }
+        for (int ch : chainOpts)
+        {
+            if (st != PRT_OK) break;
+            LaunchCfg c = cur;
+            c.chains = ch;
+            st = consider(c);
+        }
+        for (int b : perSMOpts)
+        {
+            if (st != PRT_OK) break;
+            LaunchCfg c = cur;
+            c.blocksPerSM = b;
+            st = consider(c);
+        }
+        for (int b : blockOpts)
+        {
+            if (st != PRT_OK) break;
+            LaunchCfg c = cur;
+            c.block = b;
+            st = consider(c);
+        }
+        if (!improved) break;
+    }
+    if (st != PRT_OK)
+    {
+        ctx->cfg = saved;
+        clear_graphs(ctx);
+        return st;
+    }
+    ctx->cfg = cur;
     clear_graphs(ctx);
     st = prt_clear(ctx);
     if (st != PRT_OK) return st;
     if (best)
     {
-        best->blockSize = bestCfg.block;
-        best->blocksPerSM = bestCfg.blocksPerSM;
-        best->pathsPerWave = bestCfg.pathsPerWave;
-        best->concurrentWaves = bestCfg.chains;
-        best->mray = bestMray;
+        best->blockSize = cur.block;
+        best->blocksPerSM = cur.blocksPerSM;
+        best->pathsPerWave = cur.pathsPerWave;
+        best->concurrentWaves = cur.chains;
+        best->mray = curM;
     }
     return PRT_OK;
 }
@@ -1607,7 +1672,7 @@ namespace prt_b200 {
 
 // Read-only view of a context for prt_render_noalloc (noalloc.cu).
 int ctx_noalloc_view(prt_ctx* ctx, SceneDev* scene, int* device, cudaStream_t* stream, int* numSMs, LaunchCfg* cfg,
-                     float* sky, bool* albedo)
+                     float* sky, bool* albedo, bool* nee)
 {
     if (!ctx->built) return fail(ctx, PRT_ESTATE, "acceleration structure not built (prt_build_accel)");
     *scene = scene_dev(ctx);
@@ -1617,6 +1682,7 @@ int ctx_noalloc_view(prt_ctx* ctx, SceneDev* scene, int* device, cudaStream_t* s
     *cfg = ctx->cfg;
     *sky = ctx->sky;
     *albedo = ctx->dAlbedo != nullptr;
+    *nee = ctx->integrator == PRT_INTEGRATOR_DIFFUSE2;
     return PRT_OK;
 }
 

@@ -268,6 +268,8 @@ int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n
                      int* fetch, int numSMs, cudaStream_t s);
 int launch_resolve_ldr(const float4* accum, uint32_t* out, int n, cudaStream_t s);
 int launch_advance_pass(int* passBase, int spp, cudaStream_t s);
+// primary rays of pass `pass` for every pixel of cam's frame (row-major)
+int launch_primary_rays(const CameraDev& cam, int pass, RayRec* out, cudaStream_t s);
 int launch_query(const SceneDev& sc, const RayRec* ray, HitRec* hit, float* pNg, cudaStream_t s);
 // fetch: a zeroed 64-bit work counter on the device
 int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int pass0, int spp, int maxDepth, float sky,

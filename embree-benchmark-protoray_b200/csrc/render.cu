@@ -33,6 +33,19 @@ __device__ __forceinline__ void morton8x8(int m, int& x, int& y)
     y = ((m >> 1) & 1) | ((m >> 2) & 2) | ((m >> 3) & 4);
 }
 
+// Pixel of item rr (< tilesX * tilesY * 64) of one pass of a wave: 8x8 tiles
+// in row order, Morton order inside a tile (image/morton.cpp's tables).
+// Returns false for items past the frame's right or bottom edge.
+__device__ __forceinline__ bool wave_item_pixel(int rr, int tilesX, int W, int H, int& x, int& y)
+{
+    int tile = rr >> 6;
+    int mx, my;
+    morton8x8(rr & 63, mx, my);
+    x = (tile % tilesX) * 8 + mx;
+    y = (tile / tilesX) * 8 + my;
+    return x < W && y < H;
+}
+
 __device__ __forceinline__ PathRec load_path(const PathRec* q, int i)
 {
     const float4* p = reinterpret_cast<const float4*>(q + i);
@@ -154,13 +167,8 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
                 if (kFirst)
                 {
                     int pass = i / perPass;
-                    int rr = i - pass * perPass;
-                    int tile = rr >> 6;
-                    int mx, my;
-                    morton8x8(rr & 63, mx, my);
-                    int x = (tile % a.tilesX) * 8 + mx;
-                    int y = (tile / a.tilesX) * 8 + my;
-                    if (x >= W || y >= H)
+                    int x, y;
+                    if (!wave_item_pixel(i - pass * perPass, a.tilesX, W, H, x, y))
                     {
                         ok = false;
                     }
@@ -349,13 +357,8 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
                 if (kFirst)
                 {
                     int pass = i / perPass;
-                    int rr = i - pass * perPass;
-                    int tile = rr >> 6;
-                    int mx, my;
-                    morton8x8(rr & 63, mx, my);
-                    int x = (tile % a.tilesX) * 8 + mx;
-                    int y = (tile / a.tilesX) * 8 + my;
-                    if (x >= W || y >= H)
+                    int x, y;
+                    if (!wave_item_pixel(i - pass * perPass, a.tilesX, W, H, x, y))
                     {
                         ok = false;
                     }
@@ -824,13 +827,9 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
                     long long local = gi - s_begin[req];
                     int perPass = R.tilesX * R.tilesY * 64;
                     int pass = (int)(local / perPass);
-                    int rr = (int)(local - (long long)pass * perPass);
-                    int tile = rr >> 6;
-                    int mx, my;
-                    morton8x8(rr & 63, mx, my);
-                    int x = (tile % R.tilesX) * 8 + mx;
-                    int y = (tile / R.tilesX) * 8 + my;
-                    if (x >= R.cam.width || y >= R.cam.height)
+                    int x, y;
+                    if (!wave_item_pixel((int)(local - (long long)pass * perPass), R.tilesX, R.cam.width,
+                                         R.cam.height, x, y))
                     {
                         ok = false;
                     }
@@ -999,6 +998,40 @@ int launch_resolve_ldr(const float4* accum, uint32_t* out, int n, cudaStream_t s
 {
     if (n <= 0) return 0;
     k_resolve_ldr<<<(n + 255) / 256, 256, 0, s>>>(accum, out, n);
+    return 1;
+}
+
+namespace {
+
+// The primary rays of one pass, written per pixel (row-major) as 32-byte ray
+// records (org, tnear 0, dir, tfar FLT_MAX): the wave item -> pixel mapping,
+// RNG seeding and camera_ray of the bounce kernels' first depth, exposed so
+// the generated rays can be compared with a reference one by one.
+__global__ void k_primary_rays(CameraDev cam, int tilesX, int tilesY, int pass, RayRec* out)
+{
+    const int perPass = tilesX * tilesY * 64;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < perPass; i += gridDim.x * blockDim.x)
+    {
+        int x, y;
+        if (!wave_item_pixel(i, tilesX, cam.width, cam.height, x, y)) continue;
+        const int pixel = x + y * cam.width;
+        uint32_t rng = rng_seed(pass, pixel);
+        float3 org, dir;
+        camera_ray(cam, x, y, rng, org, dir);
+        float4* o = reinterpret_cast<float4*>(out + pixel);
+        o[0] = make_float4(org.x, org.y, org.z, 0.0f);
+        o[1] = make_float4(dir.x, dir.y, dir.z, FLT_MAX);
+    }
+}
+
+} // namespace
+
+int launch_primary_rays(const CameraDev& cam, int pass, RayRec* out, cudaStream_t s)
+{
+    const int tilesX = (cam.width + 7) / 8, tilesY = (cam.height + 7) / 8;
+    const int perPass = tilesX * tilesY * 64;
+    if (perPass <= 0) return 0;
+    k_primary_rays<<<std::min((perPass + 255) / 256, 4096), 256, 0, s>>>(cam, tilesX, tilesY, pass, out);
     return 1;
 }
 

@@ -2,8 +2,8 @@
 // render/device_cuda.{h,cpp} so that `protoray render ... -dev b200` runs the
 // reference's own render loop on the B200 path tracer.  It is written against
 // the reference's headers (Device, Props, ThinLensCamera, Surface) and the C
-// ABI in include/prt_b200.h; INTEGRATION.md shows the one-line device
-// selection in main/render/render.cpp.
+// ABI in include/prt_b200.h; main/render/render.cpp selects it with one
+// more `-dev` branch (render.cpp:200-214).
 #pragma once
 
 #include <cstring>

@@ -34,7 +34,7 @@ EXPORTS = [
     "prt_init_frame", "prt_clear", "prt_read_accum", "prt_read_ldr",
     "prt_render", "prt_render_profile", "prt_set_pass", "prt_get_pass", "prt_query_ray",
     "prt_intersect", "prt_occluded", "prt_render_backward", "prt_render_replay",
-    "prt_render_batch", "prt_read_accel", "prt_read_counters", "prt_debug_fail_allocations", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count",
+    "prt_render_batch", "prt_read_accel", "prt_read_counters", "prt_debug_fail_allocations", "prt_autotune", "prt_set_tune", "prt_get_tune", "prt_render_noalloc", "prt_launch_count", "prt_primary_rays",
     "prt_soup_load_obj", "prt_soup_info", "prt_soup_triangles", "prt_soup_material_name", "prt_soup_free",
     "prt_build_mesh", "prt_build_mesh_soup", "prt_read_built_mesh", "prt_save_built_mesh",
 ]
@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
         "prt_get_tune": (ip, [vp, C.POINTER(Tune)]),
         "prt_render_noalloc": (ip, [vp, C.POINTER(Camera), ip, ip, ip, ip, ip, vp, C.POINTER(C.c_longlong)]),
         "prt_launch_count": (C.c_longlong, [vp]),
+        "prt_primary_rays": (ip, [vp, ip, vp, vp]),
         "prt_soup_load_obj": (ip, [C.c_char_p, ip, C.POINTER(vp), C.c_char_p, ip]),
         "prt_soup_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "prt_soup_triangles": (vp, [vp]),
@@ -380,6 +381,11 @@ class Context:
         """rays_dev / hits_dev: device tensors of n x 8 / n x 4 float32."""
         self._check(self.L.prt_intersect(self.h, _ptr(rays_dev), _ptr(hits_dev), n, stream or None), "prt_intersect")
 
+    def primary_rays(self, pass_: int, rays_dev, stream: int = 0):
+        """rays_dev: device tensor of (H*W) x 8 float32, filled row-major with
+        the camera rays of pass `pass_` (prt_primary_rays)."""
+        self._check(self.L.prt_primary_rays(self.h, pass_, _ptr(rays_dev), stream or None), "prt_primary_rays")
+
     def occluded(self, rays_dev, out_dev, n: int, stream: int = 0):
         self._check(self.L.prt_occluded(self.h, _ptr(rays_dev), _ptr(out_dev), n, stream or None), "prt_occluded")
 
@@ -388,6 +394,12 @@ class Context:
         self._check(self.L.prt_autotune(self.h, spp, max_depth, C.byref(t)), "prt_autotune")
         return {"blockSize": t.blockSize, "blocksPerSM": t.blocksPerSM, "pathsPerWave": t.pathsPerWave,
                 "concurrentWaves": t.concurrentWaves, "mray": t.mray}
+
+    def get_tune(self) -> Dict[str, int]:
+        t = Tune()
+        self._check(self.L.prt_get_tune(self.h, C.byref(t)), "prt_get_tune")
+        return {"blockSize": t.blockSize, "blocksPerSM": t.blocksPerSM, "pathsPerWave": t.pathsPerWave,
+                "concurrentWaves": t.concurrentWaves}
 
     def set_tune(self, block: int, per_sm: int, paths_per_wave: int, concurrent_waves: int = 0):
         t = Tune(block, per_sm, paths_per_wave, concurrent_waves, 0.0)

@@ -342,6 +342,18 @@ def spheres10m_scene(seed: int = 2, count: int = 2000) -> Tuple[Mesh, View]:
     return mesh, default_view(mesh)
 
 
+def field_view(mesh: Mesh) -> View:
+    """Camera on the front face of a scene's bounding box (x/y centre, z at
+    the box's far side), looking down -z with a 45-degree vertical field of
+    view: for the 10M-triangle icosphere field, about 47% of the primary rays
+    hit (12% from the default view outside the box)."""
+    lo = mesh.positions.min(axis=0)
+    hi = mesh.positions.max(axis=0)
+    c = 0.5 * (lo + hi)
+    return View((float(c[0]), float(c[1]), float(hi[2])), angleX=0.0, angleY=0.0,
+                fovY=float(np.float32(math.radians(45.0))), radius=0.0, focus=float(hi[2] - lo[2]))
+
+
 def batch_scene(k: int, seed: int = 100) -> Tuple[Mesh, View]:
     """Eight seeded scenes of 10K-2M tris for the uneven-batch workload."""
     rng = np.random.default_rng(seed + k)

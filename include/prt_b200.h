@@ -192,6 +192,14 @@ int prt_get_pass(prt_ctx* ctx, int* pass);
 /* p and Ng (nullable) receive the hit point and the geometric normal facing the ray. */
 int prt_query_ray(prt_ctx* ctx, const prt_ray* ray, prt_hit* hit, float p[3], float Ng[3]);
 
+/* Primary rays of pass `pass` for every pixel of the frame (width*height ray
+ * records, row-major, device pointer): the camera rays the renderer traces
+ * first, with the pixel jitter and lens samples of RandomSampler.init(pass,
+ * pixel) (generateRaysKernel, render/diffuse_renderer_cuda.cu:27-59;
+ * RendererSingle::renderTile, render/renderer_single.h:107-124); tnear 0,
+ * tfar FLT_MAX.  Needs a camera and a frame. */
+int prt_primary_rays(prt_ctx* ctx, int pass, prt_ray* rays, void* stream);
+
 /* --- intersector seam (IntersectorStreamCuda, core/intersector_stream_cuda.h:32-33) --- */
 /* Closest hit for n rays (device pointers); misses get t = -1. */
 int prt_intersect(prt_ctx* ctx, const prt_ray* rays, prt_hit* hits, int n, void* stream);
@@ -237,8 +245,14 @@ int prt_read_counters(prt_ctx* ctx, long long* out, int n, int reset);
 int prt_debug_fail_allocations(long long afterCount);
 
 /* --- launch configuration --- */
-/* Times candidate bounce-kernel configurations on the current scene/frame
- * and keeps the fastest for later renders. */
+/* Tunes the bounce kernels' launch configuration (paths per wave = queue
+ * size, concurrent waves, resident blocks per SM, block size) for the current
+ * scene, frame and camera by timing renders of `spp` passes at `maxDepth`:
+ * coordinate descent from the current configuration, one parameter at a time,
+ * a candidate replacing the incumbent only when it is more than 1% faster.
+ * Keeps the winner for later renders (see prt_get_tune), then clears the frame
+ * and the pass counter.  The renders it times are the caller's workload, so a
+ * call costs about 20-40 renders of it. */
 int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best);
 int prt_set_tune(prt_ctx* ctx, const prt_tune* tune);
 int prt_get_tune(prt_ctx* ctx, prt_tune* tune);
@@ -247,15 +261,18 @@ int prt_get_tune(prt_ctx* ctx, prt_tune* tune);
 /* Renders passes [pass0, pass0+spp) of ctx's built scene through `cam` into
  * the caller's device buffer `accum` (width*height*4 floats: sum r, g, b,
  * weight; added to, not cleared) and returns the closest-hit query count in
- * `rays` (nullable).  It allocates nothing: for callers that cannot allocate
- * device memory at render time (an application that owns the GPU's memory
- * through its own pool, or a frame loop that cannot afford cudaMalloc's
- * implicit synchronisation).  Its path queues live in one fixed 36 MiB device
- * array per GPU, so frames are limited to 524288 pixels after rounding up to
- * 8x8 tiles (larger ones return PRT_EINVAL).  All calls on a device share that
- * array: calls that overlap on the GPU race, so serialise them.  The first
- * call on a device resolves the array's address; make it before any stream
- * capture. */
+ * `rays` (nullable).  It uses the context's integrator (diffuse or diffuse2),
+ * sky and per-triangle albedo, like prt_render.  It allocates nothing: for
+ * callers that cannot allocate device memory at render time (an application
+ * that owns the GPU's memory through its own pool, or a frame loop that cannot
+ * afford cudaMalloc's implicit synchronisation).  Its path queues live in one
+ * fixed 40 MiB device array per GPU, so frames are limited to 524288 pixels
+ * after rounding up to 8x8 tiles (larger ones return PRT_EINVAL).  `accum`
+ * must be 16-byte aligned device (or managed) memory of the context's GPU,
+ * else PRT_EINVAL.  All calls on a device share that array: calls that overlap
+ * on the GPU race, so serialise them.  The first call in a CUDA context of a
+ * device resolves the array's address there; make it before any stream
+ * capture.  The caller's current device is restored on return. */
 int prt_render_noalloc(prt_ctx* ctx, const prt_camera* cam, int width, int height, int pass0, int spp, int maxDepth,
                        float* accum, long long* rays);
 

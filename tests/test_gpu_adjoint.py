@@ -55,9 +55,10 @@ def test_adjoint_matches_oracle_and_fd(setup, small_oracle, oracle_mod):
     dimg = (2.0 * (img - target)).detach().cpu().numpy().astype(np.float64)
     cam = oracle_mod.Oracle().camera(view, W, H)
     o_alb, o_sky = small_oracle.render_backward(cam, W, H, 0, spp, depth, alb, sky0, dimg / spp)
+    # every one of the 200 largest gradients within 1e-2 (observed: at most 2e-5)
     top = np.argsort(-np.abs(o_alb))[:200]
     rel = np.abs(g_alb[top] - o_alb[top]) / np.maximum(np.abs(o_alb[top]), 1e-12)
-    assert np.median(rel) < 1e-3 and np.mean(rel < 1e-2) > 0.97, (np.median(rel), np.mean(rel < 1e-2))
+    assert np.median(rel) < 1e-4 and np.all(rel < 1e-2), (np.median(rel), rel.max())
     assert abs(g_sky - o_sky) <= 1e-2 * abs(o_sky)
     np.testing.assert_allclose(np.linalg.norm(g_alb), np.linalg.norm(o_alb), rtol=1e-2)
 

@@ -25,13 +25,32 @@ def _decode(nodes):
     return origin, scale, imask, child, tbase, meta, qlo, qhi
 
 
+def _chain(n, ratio):
+    """n nested triangles whose sizes shrink geometrically (ratio per step)
+    around one point, so that SAH splits peel the largest off one by one."""
+    s = ratio ** np.arange(n, dtype=np.float64)
+    c = np.stack([0.1 * s, 0.05 * s, 0 * s], axis=1)
+    shape = np.array([[-0.5, -0.3, 0.0], [0.5, -0.3, 0.1], [0.0, 0.6, -0.1]])
+    pos = (c[:, None, :] + s[:, None, None] * shape[None]).reshape(-1, 3).astype(np.float32)
+    return pos, np.arange(3 * n, dtype=np.int32).reshape(n, 3)
+
+
 @pytest.mark.parametrize("scene,leaf,high", [("small", 1, 1), ("small", 3, 1), ("batch3", 1, 1), ("batch3", 2, 1),
                                              ("one", 1, 1), ("two", 1, 1), ("two", 3, 1), ("small", 1, 0),
-                                             ("batch3", 2, 0)])
+                                             ("batch3", 2, 0), ("dup", 1, 1), ("dup", 1, 0), ("chain200", 1, 1),
+                                             ("chain1000", 1, 1), ("chain1000", 2, 0)])
 def test_bvh_structure(scene, leaf, high, small):
     import prt
     import scenes
-    if scene == "small":
+    if scene == "dup":
+        # 5000 copies of one triangle: every centroid in one bin, across
+        # several 4096-triangle chunks (the split by position)
+        pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+        idx = np.zeros((5000, 3), np.int32) + np.array([0, 1, 2], np.int32)
+    elif scene.startswith("chain"):
+        n = int(scene[5:])
+        pos, idx = _chain(n, 0.8 if n <= 256 else 0.95)
+    elif scene == "small":
         mesh, _ = small
         pos, idx = mesh.positions, mesh.indices
     elif scene == "batch3":

@@ -181,16 +181,21 @@ def c_stdout_to_stderr():
         os.close(saved)
 
 
-def cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, scene="terrain"):
+def cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, scene="terrain", accel=1):
     with c_stdout_to_stderr():
-        return _cpu_reference_run(steps, warmup, frames_per_step, sample_seconds, scene)
+        return _cpu_reference_run(steps, warmup, frames_per_step, sample_seconds, scene, accel)
 
 
-def _cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, scene="terrain"):
+CPU_BVH = {1: "project 8-wide AVX2 BVH with 4-triangle leaves (bvh8.triangle4 class) standing in for Embree 3 (absent)",
+           2: "project scalar binary FP32 BVH standing in for Embree 3 (absent)"}
+
+
+def _cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, scene="terrain", accel=1):
     """Times the reference's own diffuseStream renderer (oracle/_ref) on the
     host cores; one step = `frames_per_step` 1-spp frames.  scene "terrain":
     1920x1080, maxDepth 5; "spheres10m": the 10.24M-triangle icosphere field
-    from its in-field camera, 1920x1080, maxDepth 8."""
+    from its in-field camera, 1920x1080, maxDepth 8.  accel 1: the 8-wide
+    AVX2 BVH; 2: the scalar binary BVH."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     import scenes
@@ -209,17 +214,17 @@ def _cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, sc
     R = oracle.Reference()
     rs = R.open(path)
     tb = time.perf_counter()
-    rs.build(1)
+    rs.build(accel)
     build_s = time.perf_counter() - tb
     cores = int(os.environ.get("PRT_REF_THREADS", "0")) or (os.cpu_count() or 1)
     for _ in range(warmup):
-        rs.render("diffuseStream", view, w, h, frames_per_step, depth, accel=1, want_sums=False)
+        rs.render("diffuseStream", view, w, h, frames_per_step, depth, accel=accel, want_sums=False)
     rays = 0.0
     secs = 0.0
     t0 = time.perf_counter()
     n = 0
     while n < steps:
-        _, st = rs.render("diffuseStream", view, w, h, frames_per_step, depth, accel=1, want_sums=False)
+        _, st = rs.render("diffuseStream", view, w, h, frames_per_step, depth, accel=accel, want_sums=False)
         rays += st["rays"]
         secs += st["seconds"]
         n += 1
@@ -231,7 +236,7 @@ def _cpu_reference_run(steps, warmup, frames_per_step=1, sample_seconds=None, sc
     except OSError:
         pass
     return {"value": rays / 1e6 / secs, "rays": rays, "seconds": secs, "wall": wall, "frames": n * frames_per_step,
-            "cores": cores, "cpu": cpu_model(), "build_s": build_s}
+            "cores": cores, "cpu": cpu_model(), "build_s": build_s, "bvh": CPU_BVH[accel]}
 
 
 def cpu_model():
@@ -252,9 +257,9 @@ def run_reference(args):
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libprotoray_ref.so was not built"}))
         return 0
-    sample = (f"reference diffuseStream renderer (stream 2048, AVX2, GCC -O3) with the project FP32 SAH BVH "
-              f"standing in for Embree 3 (absent); terrain scene 1920x1080, {r['frames']} frames x 1 spp, "
-              f"maxDepth {DEPTH}; {r['cpu']}")
+    r2 = cpu_reference_run(args.steps, 1, accel=2)
+    sample = (f"reference diffuseStream renderer (stream 2048, AVX2, GCC -O3) with the {r['bvh']}; terrain scene "
+              f"1920x1080, {r['frames']} frames x 1 spp, maxDepth {DEPTH}; {r['cpu']}")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(r["value"], 3), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * r["seconds"] / max(1, r["frames"]), 3),
@@ -266,6 +271,7 @@ def run_reference(args):
         "cpu_baseline": {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(r["value"], 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "scalar_bvh": {"value": round(r2["value"], 3), "unit": UNIT, "bvh": r2["bvh"], "frames": r2["frames"]},
     }
     print(json.dumps(line))
     return 0
@@ -440,8 +446,8 @@ def run_c2(prt, torch, device, steps, warmup, cpu_seconds):
             out["cpu_baseline"] = {
                 "value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "reference",
                 "build_s": round(r["build_s"], 2),
-                "sample": (f"reference diffuseStream renderer + project CPU BVH (Embree 3 absent), same scene and "
-                           f"camera, {r['frames']} frames x 1 spp, maxDepth {C2_DEPTH}, {r['wall']:.1f} s")}
+                "sample": (f"reference diffuseStream renderer with the {r['bvh']}, same scene and camera, "
+                           f"{r['frames']} frames x 1 spp, maxDepth {C2_DEPTH}, {r['wall']:.1f} s")}
             out["vs_cpu"] = round(out["value"] / r["value"], 1)
     return out
 
@@ -736,9 +742,10 @@ def main():
         extras["c2"] = run_c2(prt, torch, local, args.steps, args.warmup,
                               0 if (args.no_cpu or world > 1) else args.cpu_seconds / 2)
 
-    cpu = None
+    cpu = cpu_scalar = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_run(1000, 1, sample_seconds=args.cpu_seconds)
+        cpu = cpu_reference_run(1000, 1, sample_seconds=0.7 * args.cpu_seconds)
+        cpu_scalar = cpu_reference_run(1000, 1, sample_seconds=0.3 * args.cpu_seconds, accel=2)
 
     if rank == 0:
         line = {
@@ -763,9 +770,10 @@ def main():
         if cpu is not None:
             line["cpu_baseline"] = {
                 "value": round(cpu["value"], 3), "unit": UNIT, "cores": cpu["cores"], "kind": "reference",
-                "sample": (f"reference diffuseStream renderer + project FP32 SAH BVH (Embree 3 absent), terrain "
-                           f"scene 1920x1080, {cpu['frames']} frames x 1 spp, maxDepth 5, {cpu['wall']:.1f} s; "
-                           f"{cpu['cpu']}")}
+                "sample": (f"reference diffuseStream renderer with the {cpu['bvh']}, terrain scene 1920x1080, "
+                           f"{cpu['frames']} frames x 1 spp, maxDepth 5, {cpu['wall']:.1f} s; {cpu['cpu']}"),
+                "scalar_bvh": {"value": round(cpu_scalar["value"], 3), "bvh": cpu_scalar["bvh"],
+                               "frames": cpu_scalar["frames"]}}
         line.update(extras)
         print(json.dumps(line))
     ctx.close()

@@ -241,6 +241,7 @@ class Reference:
             lib.ref_render.restype = C.c_int
             lib.ref_render.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
+            lib.ref_fast_trace.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
             lib.ref_query_ray.restype = C.c_int
             lib.ref_query_ray.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
             lib.ref_rng.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
@@ -344,7 +345,17 @@ class RefScene:
         return pos, idx
 
     def build(self, accel: int) -> float:
+        """accel: 0 = FP64 oracle BVH, 1 = 8-wide AVX2 BVH with 4-triangle
+        leaves (timing), 2 = scalar binary FP32 BVH (timing)."""
         return float(self.r.lib.ref_scene_build(self.h, accel))
+
+    def fast_trace(self, rays: np.ndarray, accel: int = 1, any_hit: bool = False) -> np.ndarray:
+        """Closest hits (n x 4: t or -1, primId bits, u, v) or occlusion flags
+        (n) of n x 8 rays through a timing BVH (accel 1 or 2)."""
+        r = np.ascontiguousarray(rays, np.float32)
+        out = np.zeros(len(r) if any_hit else (len(r), 4), np.float32)
+        self.r.lib.ref_fast_trace(self.h, accel, int(any_hit), r.ctypes.data, len(r), out.ctypes.data)
+        return out
 
     def render(self, renderer: str, view, width: int, height: int, frames: int, max_depth: int, accel: int = 0,
                want_sums: bool = True):

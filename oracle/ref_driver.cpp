@@ -10,9 +10,12 @@
 // IntersectorSingle / IntersectorStream<N> (core/intersector_single.h:23-31,
 // core/intersector_stream.h:23-31).  Their only implementations in the
 // reference are Embree 3 wrappers (accel/embree/*), and Embree is absent here,
-// so two project intersectors implement those interfaces instead:
+// so project intersectors implement those interfaces instead:
 //   * OracleIntersector: the FP64 watertight BVH of prt_oracle.c (parity);
-//   * FastIntersector:   the FP32 binned-SAH BVH of cpu_bvh32.hpp (timing).
+//   * FastIntersector over the 8-wide AVX2 BVH with 4-triangle leaves of
+//     cpu_bvh8.hpp (timing; the class of structure the reference asks Embree
+//     for, bvh8.triangle4), or over the scalar binary FP32 BVH of
+//     cpu_bvh32.hpp (timing, for comparison).
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -37,6 +40,7 @@
 
 #include "prt_oracle.h"
 #include "cpu_bvh32.hpp"
+#include "cpu_bvh8.hpp"
 
 using namespace prt;
 
@@ -51,6 +55,8 @@ struct SceneHandle
     std::vector<int> idx;
     or_scene* fp64 = nullptr;
     prt_oracle::Bvh32 bvh;
+    prt_oracle::Bvh8 bvh8;
+    bool bvh8Built = false;
     std::string error;
 };
 
@@ -85,12 +91,31 @@ public:
     }
 };
 
+// Closest-hit / any-hit queries of the two timing BVHs behind one interface.
+struct FastBvh
+{
+    const prt_oracle::Bvh32* b32 = nullptr;
+    const prt_oracle::Bvh8* b8 = nullptr;
+
+    bool intersect(const float org[3], const float dir[3], float& t, int& prim, float& u, float& v) const
+    {
+        return b8 ? b8->intersect(org, dir, t, prim, u, v) : b32->intersect(org, dir, t, prim, u, v);
+    }
+    bool occluded(const float org[3], const float dir[3], float t) const
+    {
+        if (b8) return b8->occluded(org, dir, t);
+        float u, v;
+        int prim;
+        return b32->intersect(org, dir, t, prim, u, v);
+    }
+};
+
 class FastIntersectorSingle : public IntersectorSingle
 {
-    const prt_oracle::Bvh32* bvh;
+    FastBvh bvh;
 
 public:
-    explicit FastIntersectorSingle(const prt_oracle::Bvh32* b) : bvh(b) {}
+    explicit FastIntersectorSingle(FastBvh b) : bvh(b) {}
 
     void intersect(Ray& ray, Hit& hit, RayStats& stats, RayHint) override
     {
@@ -98,7 +123,7 @@ public:
         float org[3] = {ray.org.x, ray.org.y, ray.org.z}, dir[3] = {ray.dir.x, ray.dir.y, ray.dir.z};
         float t = ray.far, u = 0, v = 0;
         int prim = -1;
-        if (bvh->intersect(org, dir, t, prim, u, v))
+        if (bvh.intersect(org, dir, t, prim, u, v))
         {
             ray.far = t;
             hit.primId = prim;
@@ -111,19 +136,19 @@ public:
     {
         stats.rayCount++;
         float org[3] = {ray.org.x, ray.org.y, ray.org.z}, dir[3] = {ray.dir.x, ray.dir.y, ray.dir.z};
-        float t = ray.far, u, v;
-        int prim;
-        if (bvh->intersect(org, dir, t, prim, u, v)) ray.far = 0.0f;
+        if (bvh.occluded(org, dir, ray.far)) ray.far = 0.0f;
     }
 };
 
+// The stream interface of the reference's stream renderers, one ray at a time
+// (Embree's rtcIntersectNp traverses incoherent streams ray by ray as well).
 template <int N>
 class FastIntersectorStream : public IntersectorStream<N>
 {
-    const prt_oracle::Bvh32* bvh;
+    FastBvh bvh;
 
 public:
-    explicit FastIntersectorStream(const prt_oracle::Bvh32* b) : bvh(b) {}
+    explicit FastIntersectorStream(FastBvh b) : bvh(b) {}
 
     void intersect(RayStream<N>& rays, HitStream<N>& hits, int count, RayStats& stats, RayHint) override
     {
@@ -137,7 +162,7 @@ public:
             float org[3] = {ox[i], oy[i], oz[i]}, dir[3] = {dx[i], dy[i], dz[i]};
             float t = far[i], u = 0, v = 0;
             int prim = -1;
-            if (bvh->intersect(org, dir, t, prim, u, v))
+            if (bvh.intersect(org, dir, t, prim, u, v))
             {
                 far[i] = t;
                 pid[i] = prim;
@@ -154,9 +179,7 @@ public:
         {
             float org[3] = {rays.getOrgX()[i], rays.getOrgY()[i], rays.getOrgZ()[i]};
             float dir[3] = {rays.getDirX()[i], rays.getDirY()[i], rays.getDirZ()[i]};
-            float t = rays.getFar()[i], u, v;
-            int prim;
-            if (bvh->intersect(org, dir, t, prim, u, v)) rays.getFar()[i] = 0.0f;
+            if (bvh.occluded(org, dir, rays.getFar()[i])) rays.getFar()[i] = 0.0f;
         }
     }
 };
@@ -254,21 +277,27 @@ void ref_scene_arrays(void* handle, float* pos, int* idx)
     std::memcpy(idx, h->idx.data(), sizeof(int) * h->idx.size());
 }
 
-// accel: 0 = FP64 oracle BVH, 1 = FP32 SAH BVH.  Returns build seconds.
+// accel: 0 = FP64 oracle BVH, 1 = 8-wide AVX2 BVH (4-triangle leaves),
+// 2 = scalar binary FP32 SAH BVH.  Returns build seconds.
 double ref_scene_build(void* handle, int accel)
 {
     SceneHandle* h = (SceneHandle*)handle;
     auto t0 = std::chrono::steady_clock::now();
     int nt = (int)(h->idx.size() / 3), nv = (int)(h->pos.size() / 3);
     if (accel == 0 && !h->fp64) h->fp64 = or_scene_create(h->pos.data(), nv, h->idx.data(), nt);
-    if (accel == 1 && h->bvh.nodes.empty()) h->bvh.build(h->pos.data(), h->idx.data(), nt);
+    if (accel == 1 && !h->bvh8Built)
+    {
+        h->bvh8.build(h->pos.data(), h->idx.data(), nt);
+        h->bvh8Built = true;
+    }
+    if (accel == 2 && h->bvh.nodes.empty()) h->bvh.build(h->pos.data(), h->idx.data(), nt);
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // Renders `frames` frames with a reference renderer, one sample per pixel per
 // frame as the reference's render loop does (main/render/render_window.cpp:204-256).
 //   renderer: "diffuse", "diffuseFast", "diffuse2", "diffuse2Fast", "diffuseStream", "diffuseStreamFast"
-//   accel:    0 = FP64 oracle BVH, 1 = FP32 SAH BVH
+//   accel:    0 = FP64 oracle BVH, 1 = 8-wide AVX2 BVH, 2 = scalar binary FP32 BVH
 //   view:     {pos.xyz, angleX, angleY, fovY, radius, focus}
 //   sums:     W*H*4 floats (r,g,b,weight) or NULL
 //   stats:    [0] rays, [1] seconds (sum of the renderer's own frame timers),
@@ -281,6 +310,9 @@ int ref_render(void* handle, const char* renderer, int accel, int W, int H, int 
     try
     {
         ref_scene_build(handle, accel);
+        FastBvh fast;
+        if (accel == 1) fast.b8 = &h->bvh8;
+        else fast.b32 = &h->bvh;
         std::string type(renderer);
         Props props;
         props.set("type", type);
@@ -299,7 +331,7 @@ int ref_render(void* handle, const char* renderer, int accel, int W, int H, int 
         {
             ref<IntersectorSingle> isect;
             if (accel == 0) isect = makeRef<OracleIntersector>(h->fp64);
-            else isect = makeRef<FastIntersectorSingle>(&h->bvh);
+            else isect = makeRef<FastIntersectorSingle>(fast);
             // render/renderer_factory_single.cpp (diffuse2 / diffuse2Fast)
             if (type == "diffuse2")
                 r = makeRef<RendererSingle<Diffuse2IntegratorSingle<ShadingContext, RandomSampler>, RandomSampler>>(scene, isect, props);
@@ -310,7 +342,7 @@ int ref_render(void* handle, const char* renderer, int accel, int W, int H, int 
         {
             ref<IntersectorSingle> isect;
             if (accel == 0) isect = makeRef<OracleIntersector>(h->fp64);
-            else isect = makeRef<FastIntersectorSingle>(&h->bvh);
+            else isect = makeRef<FastIntersectorSingle>(fast);
             // render/renderer_factory_single.cpp:56-59
             if (type == "diffuse")
                 r = makeRef<RendererSingle<DiffuseIntegratorSingle<ShadingContext, RandomSampler>, RandomSampler>>(scene, isect, props);
@@ -319,8 +351,8 @@ int ref_render(void* handle, const char* renderer, int accel, int W, int H, int 
         }
         else if (type == "diffuseStream" || type == "diffuseStreamFast")
         {
-            if (accel != 1) throw std::invalid_argument("stream renderers use the FP32 BVH");
-            ref<IntersectorStream<kStream>> isect = makeRef<FastIntersectorStream<kStream>>(&h->bvh);
+            if (accel == 0) throw std::invalid_argument("stream renderers use a FP32 BVH (accel 1 or 2)");
+            ref<IntersectorStream<kStream>> isect = makeRef<FastIntersectorStream<kStream>>(fast);
             // render/renderer_factory_stream.cpp:91-94 (streamTileX 64, streamTileY 2048/64)
             if (type == "diffuseStream")
                 r = makeRef<DiffuseRendererStream<ShadingContextSimd, RandomSamplerSimd, true, kStream, 64, kStream / 64>>(scene, isect, props);
@@ -394,6 +426,45 @@ int ref_query_ray(void* handle, const float ray[7], float* out)
     out[2] = p.x; out[3] = p.y; out[4] = p.z;
     out[5] = Ng.x; out[6] = Ng.y; out[7] = Ng.z;
     return 1;
+}
+
+// Closest hits (accel 1 or 2) or occlusion (any != 0) of n rays through a
+// timing BVH, for checking it against the FP64 oracle.  rays: n x 8 floats
+// (org, tnear ignored, dir, tfar); out: n x 4 floats (t or -1, primId bits,
+// u, v), or n floats (1 occluded, 0 free) for occlusion.
+void ref_fast_trace(void* handle, int accel, int any, const float* rays, int n, float* out)
+{
+    SceneHandle* h = (SceneHandle*)handle;
+    ref_scene_build(handle, accel);
+    FastBvh fast;
+    if (accel == 1) fast.b8 = &h->bvh8;
+    else fast.b32 = &h->bvh;
+    for (int i = 0; i < n; ++i)
+    {
+        const float* r = rays + 8 * (size_t)i;
+        float org[3] = {r[0], r[1], r[2]}, dir[3] = {r[4], r[5], r[6]};
+        if (any)
+        {
+            out[i] = fast.occluded(org, dir, r[7]) ? 1.0f : 0.0f;
+            continue;
+        }
+        float t = r[7], u = 0, v = 0;
+        int prim = -1;
+        float* o = out + 4 * (size_t)i;
+        if (fast.intersect(org, dir, t, prim, u, v))
+        {
+            o[0] = t;
+            std::memcpy(&o[1], &prim, 4);
+            o[2] = u;
+            o[3] = v;
+        }
+        else
+        {
+            o[0] = -1.0f;
+            std::memcpy(&o[1], &prim, 4);
+            o[2] = o[3] = 0.0f;
+        }
+    }
 }
 
 // `protoray build` of the reference, split at its two seams so that each can

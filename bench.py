@@ -350,6 +350,51 @@ def run_batch(prt, torch, device, reps=2):
            "requests": len(work), "rays": int(best_b["ray"])}
     out["speedup"] = round(out["batched_mray"] / out["sequential_mray"], 3)
     out["speedup_vs_calls"] = round(out["batched_mray"] / out["sequential_calls_mray"], 3)
+
+    # By request size class (paths = width x height x spp): each class's
+    # requests as one batched launch vs one prt_render call per request, device
+    # time and host wall time (calls include their launch and completion wait).
+    classes = {"small (< 1M paths)": lambda n: n < (1 << 20),
+               "medium (1M-8M paths)": lambda n: (1 << 20) <= n < (1 << 23),
+               "large (>= 8M paths)": lambda n: n >= (1 << 23)}
+    by_class = {}
+    for name, pick in classes.items():
+        idx = [i for i, q in enumerate(work) if pick(q["width"] * q["height"] * q["spp"])]
+        if not idx:
+            continue
+        sub = [reqs[i] for i in idx]
+        batcher.render_batch(sub)   # warm-up (graph capture)
+        b_best, b_wall = None, None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = batcher.render_batch(sub)
+            wall = time.perf_counter() - t0
+            if b_best is None or st["ms"] < b_best["ms"]:
+                b_best, b_wall = st, wall
+
+        def calls():
+            ms, rays = 0.0, 0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for i in idx:
+                q = work[i]
+                c = ctxs[q["scene"]]
+                c.init_frame(q["width"], q["height"])
+                c.set_view(views[q["scene"]], q["width"], q["height"])
+                st = c.render(q["spp"], q["maxDepth"], accumulate=False)
+                ms += st["ms"]
+                rays += st["ray"]
+            return ms, rays, time.perf_counter() - t0
+
+        calls()
+        c_best = min((calls() for _ in range(reps)), key=lambda x: x[0])
+        by_class[name] = {"requests": len(idx), "rays": int(b_best["ray"]),
+                          "batched_mray": round(b_best["mray"], 2), "calls_mray": round(c_best[1] / 1e3 / c_best[0], 2),
+                          "speedup_vs_calls": round(b_best["mray"] / (c_best[1] / 1e3 / c_best[0]), 3),
+                          "batched_wall_ms": round(1e3 * b_wall, 2), "calls_wall_ms": round(1e3 * c_best[2], 2),
+                          "speedup_vs_calls_wall": round(c_best[2] / b_wall, 3)}
+    out["by_size_class"] = by_class
     for c in ctxs:
         c.close()
     return out

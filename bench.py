@@ -52,6 +52,21 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def profile_issue():
+    """Warp instructions per closest-hit query of the bounce kernel on the
+    headline workload, from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_bounce_issue_terrain1080p.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("warp_inst_per_ray="):
+            try:
+                return float(line.split("=", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
 def profile_traffic():
     """DRAM bytes per ray of the bounce kernel from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "k_bounce_terrain1080p.txt")
@@ -659,6 +674,9 @@ def main():
     ap.add_argument("--width", type=int, default=W, help="smaller frames are for profiling captures only")
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--profile-depths", action="store_true",
+                    help="render the headline frame once through prt_render_profile (one launch per bounce and "
+                         "wave, no graph), print rays and ms per bounce, and exit (for profiler captures)")
     ap.add_argument("--kernel-tour", action="store_true",
                     help="launch every kernel family once on small cases (for profiler captures) and exit")
     args = ap.parse_args()
@@ -674,6 +692,17 @@ def main():
         torch.cuda.set_device(0)
         return run_kernel_tour(prt, torch, 0)
     W, H, SPP = args.width, args.height, args.spp
+    if args.profile_depths:
+        import prt
+        import scenes
+        mesh, view = scenes.terrain_scene()
+        c, _ = make_ctx(prt, mesh, 0)
+        c.init_frame(W, H)
+        c.set_view(view, W, H)
+        ms, rays = c.render_profile(SPP, DEPTH)
+        print(json.dumps({"ms_per_depth": [round(float(x), 4) for x in ms], "rays_per_depth": [int(x) for x in rays]}))
+        c.close()
+        return 0
 
     rank, world, local = dist_env()
     import torch
@@ -778,6 +807,22 @@ def main():
                 "per": "render step (the k_bounce launches of one 64-spp frame, >99% of its device time)"}
     if tr is not None:
         roofline["traffic_bytes_per_ray"] = tr
+    # The binding limit of the bounce kernel is instruction issue, not HBM:
+    # warp instructions per ray (ncu smsp__inst_executed of the bounce
+    # launches of one wave, committed summary) x rays of a step, over the SM
+    # issue peak (SMs x 4 schedulers x 1 warp instruction per clock at the
+    # median SM clock sampled during the timed steps) x the step's device time.
+    ipr = profile_issue()
+    roofline_issue = None
+    if ipr is not None:
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clocks.summary().get("sm_mhz") or 1965.0
+        inst_rate = ipr * rays_per_step / (ms_max / args.steps / 1e3)
+        peak_rate = sms * 4 * mhz * 1e6
+        roofline_issue = {"bound": "issue", "achieved": round(inst_rate / 1e12, 4), "peak": round(peak_rate / 1e12, 4),
+                          "unit": "T warp-inst/s", "frac": round(inst_rate / peak_rate, 4),
+                          "warp_inst_per_ray": ipr, "sms": sms, "sm_mhz": mhz,
+                          "per": "render step (device time of the whole step; the bounce kernels are >99% of it)"}
 
     extras = {}
     if rank == 0 and not args.no_extras:
@@ -810,6 +855,7 @@ def main():
                     "d2h_bytes_per_step": W * H * 16},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "roofline_issue": roofline_issue,
             "clocks": clocks.summary(),
         }
         if cpu is not None:

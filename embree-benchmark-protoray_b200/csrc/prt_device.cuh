@@ -430,8 +430,10 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
 // slot order, so the triangle of leaf slot j is triBase + popc(leafMask below j).
 // Returns internal hits at bits 24 + (slot ^ octinv) as node_hits does, leaf
 // hits as slot bits 0..7, and the node's leaf-slot mask in leafMask.
+// octinv: the octant code that orders the internal hit bits (the ray's own in
+// per-lane traversal; one shared by a warp in packet traversal).
 __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q, float tnear, float tfar,
-                                               uint32_t& leafMask)
+                                               uint32_t& leafMask, uint32_t octinv)
 {
     float px = __uint_as_float(q[0].x), py = __uint_as_float(q[0].y), pz = __uint_as_float(q[0].z);
     uint32_t e = q[0].w;
@@ -473,7 +475,7 @@ __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q,
     leafMask = ne & ~imask;
     // internal hits: bit slot -> bit slot ^ octinv (three conditional swaps)
     uint32_t in8 = c8 & imask;
-    const uint32_t o = r.octinv;
+    const uint32_t o = octinv;
     uint32_t sw = ((in8 & 0x55u) << 1) | ((in8 >> 1) & 0x55u);
     in8 = (o & 1u) ? sw : in8;
     sw = ((in8 & 0x33u) << 2) | ((in8 >> 2) & 0x33u);
@@ -706,7 +708,7 @@ __device__ __forceinline__ void trav_visit(TravState& s, const SceneDev& sc, con
     uint32_t hits;
     if (PRT_LEAF1_HITS)
     {
-        hits = node_hits1(r, q, tnear, s.tHit, leafMask);
+        hits = node_hits1(r, q, tnear, s.tHit, leafMask, r.octinv);
     }
     else
     {

@@ -291,6 +291,148 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
     }
 }
 
+// Primary rays as warp packets (trees with one-triangle leaves).  A warp takes
+// 32 consecutive wave items, half of an 8x8 tile (an 8x4 pixel block of one
+// pass), and traverses the tree once for all of them: every lane tests its own
+// ray against the node all lanes are at (one broadcast load of the node), the
+// node's child hits are OR-ed over the warp, and the children are visited in
+// the order of one ray octant shared by the warp, from a stack in shared
+// memory that the warp shares.  Each lane culls with its own closest hit and
+// tests the triangles of the leaves its own ray hits, so its result is its
+// closest hit, the same as per-lane traversal gives (exact ties go to the
+// lower primitive id either way).  Camera rays of a small pixel block visit
+// nearly the same nodes, so the lanes stay busy together where the per-lane
+// traversal of k_bounce runs 20 of 32 lanes per instruction at this depth.
+#ifndef PRT_PACKET_PRIMARY
+#define PRT_PACKET_PRIMARY 1
+#endif
+constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build accepts (32)
+
+template <bool kAlbedo>
+__global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_primary_packet(WaveArgs a)
+{
+    extern __shared__ uint2 s_packet[];
+    uint2* stk = s_packet + (threadIdx.x >> 5) * kPacketStack;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const int W = a.cam.width, H = a.cam.height;
+    const int perPass = a.tilesX * a.tilesY * 64;
+    const int total = a.passes * perPass;
+    const int pass0 = *a.passBase + a.passOffset;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(a.rays, (unsigned long long)a.passes * (unsigned long long)W * (unsigned long long)H);
+    const bool final = a.maxDepth == 0;
+    for (;;)
+    {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&a.fetch[0], 32);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= total) break;
+        const int i = base + (int)lane;
+        bool valid = false;
+        int pixel = 0;
+        uint32_t rng = 0;
+        float3 org = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f);
+        if (i < total)
+        {
+            const int pass = i / perPass;
+            int x, y;
+            if (wave_item_pixel(i - pass * perPass, a.tilesX, W, H, x, y))
+            {
+                valid = true;
+                pixel = x + y * W;
+                rng = rng_seed(pass0 + pass, pixel);
+                camera_ray(a.cam, x, y, rng, org, dir);
+            }
+        }
+        const unsigned vmask = __ballot_sync(FULL, valid);
+        if (!vmask) continue;
+        TravRay r;
+        trav_setup(r, org, dir);
+        const uint32_t woct = __shfl_sync(FULL, r.octinv, __ffs(vmask) - 1);
+        float tHit = FLT_MAX;
+        int primHit = 0x7fffffff;
+        int triHit = -1;
+        if (a.scene.hasRoot)
+        {
+            int sp = 0;
+            uint2 ng = make_uint2(0u, 0x80000000u);   // the root: one internal child at base 0
+            for (;;)
+            {
+                const uint32_t b = 31u - __clz(ng.y & 0xff000000u);
+                ng.y &= ~(1u << b);
+                const uint32_t slot = (b - 24u) ^ woct;
+                const uint32_t nodeIdx = ng.x + __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
+                if ((ng.y & 0xff000000u) && sp < kPacketStack)
+                {
+                    if (lane == 0) stk[sp] = ng;
+                    ++sp;
+                }
+                const uint4* qp = reinterpret_cast<const uint4*>(a.scene.nodes + nodeIdx);
+                uint4 q[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
+                uint32_t leafMask = 0;
+                const uint32_t hits = valid ? node_hits1(r, q, 0.0f, tHit, leafMask, woct) : 0u;
+                // this lane's leaf triangles (leaf slot j -> triBase + rank of j among the leaf slots)
+                uint32_t lb = hits & 0xffu;
+                while (lb)
+                {
+                    const uint32_t bit = __ffs(lb) - 1u;
+                    lb &= lb - 1u;
+                    const int ti = (int)(q[1].y + __popc(leafMask & ((1u << bit) - 1u)));
+                    const float4* tp = reinterpret_cast<const float4*>(a.scene.tris + ti);
+                    const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+                    const int prim = __float_as_int(v0.w);
+                    float t, u, v;
+                    if (tri_test(r, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), 0.0f, tHit,
+                                 prim, primHit, t, u, v))
+                    {
+                        tHit = t;
+                        primHit = prim;
+                        triHit = ti;
+                    }
+                }
+                ng = make_uint2(q[1].x, __reduce_or_sync(FULL, hits & 0xff000000u) | (q[0].w >> 24));
+                if (!(ng.y & 0xff000000u))
+                {
+                    if (sp == 0) break;
+                    __syncwarp();
+                    ng = stk[--sp];
+                    __syncwarp();
+                }
+            }
+        }
+        // shade / append / accumulate, as k_bounce does at depth 0
+        bool cont = false;
+        float contrib = 0.f;
+        float thr = kAlbedo ? 1.0f : a.thrConst;
+        if (valid)
+        {
+            if (triHit < 0)
+            {
+                contrib = __fmul_rn(thr, a.sky);
+            }
+            else if (!final)
+            {
+                if (kAlbedo) thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + primHit) : 0.8f);
+                diffuse_bounce(a.scene.tris, triHit, org, dir, tHit, rng);
+                cont = true;
+            }
+        }
+        const int o = warp_append(cont, &a.counts[1]);
+        if (cont)
+        {
+            store_path(a.qout, o, org, pixel, dir, rng);
+            if (kAlbedo) __stcs(a.thrOut + o, thr);
+        }
+        else if (valid)
+        {
+            red_add_v4(a.accum + pixel, contrib, contrib, contrib, 1.0f);
+        }
+    }
+}
+
 // Bounce kernel of the next-event-estimation integrator
 // (render/diffuse2_integrator_single.h:41-90, render/diffuse2_renderer_cuda.cu:63-239).
 // A lane takes a path's extension ray; at a hit before maxDepth it samples a
@@ -942,6 +1084,17 @@ int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs
             if (albedo) go(k_bounce_nee<false, true>);
             else go(k_bounce_nee<false, false>);
         }
+        return 1;
+    }
+    if (depth == 0 && PRT_PACKET_PRIMARY && a.scene.leafTris == 1)
+    {
+        const size_t pshmem = sizeof(uint2) * kPacketStack * (cfg.block / 32);
+        auto goPacket = [&](auto kernel) {
+            int grid = grid_for(kernel, cfg.block, pshmem, numSMs, cfg);
+            kernel<<<grid, cfg.block, pshmem, s>>>(a);
+        };
+        if (albedo) goPacket(k_primary_packet<true>);
+        else goPacket(k_primary_packet<false>);
         return 1;
     }
     if (depth == 0)

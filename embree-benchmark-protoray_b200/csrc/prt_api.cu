@@ -171,6 +171,7 @@ SceneDev scene_dev(const prt_ctx* ctx)
     s.triCount = ctx->nt;
     s.hasRoot = ctx->bvh.nodeCount > 0 ? 1 : 0;
     s.leafTris = ctx->bvh.leafMax;
+    s.deferTris = ctx->bvh.leafMax == 1 && ctx->nt < kDeferMaxTris ? 1 : 0;
     return s;
 }
 
@@ -1251,7 +1252,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
         b.maxDepth = q.maxDepth;
         b.pathBegin = total;
         total += (long long)b.tilesX * b.tilesY * 64 * q.spp;
-        if (b.scene.leafTris != 1) leaf1 = 0;
+        if (!b.scene.deferTris) leaf1 = 0;
         maxDepth = std::max(maxDepth, q.maxDepth);
         key << ":" << (const void*)q.scene << "," << q.width << "x" << q.height << "," << q.spp << "," << q.maxDepth
             << "," << (const void*)q.accum;

@@ -193,7 +193,12 @@ struct SceneDev
     int triCount;
     int hasRoot;           // 0 for an empty scene
     int leafTris;          // most triangles in one leaf (the build's leaf size)
+    int deferTris;         // one-triangle leaves and fewer than 2^27 triangles: deferred triangle tests
 };
+
+// Leaf-order triangle indices the deferred-test queue can hold (27 bits; the
+// other 5 bits of a queue entry hold the owner lane).
+constexpr int kDeferMaxTris = 1 << 27;
 
 // Per-ray constants for traversal.
 struct TravRay
@@ -671,10 +676,9 @@ constexpr uint32_t kTriQMask = kTriQCap - 1;
 struct TriQueue
 {
     unsigned long long key[32];   // per owner lane: (t bits << 32) | primitive id
-    uint32_t tri[kTriQCap];       // leaf-order triangle index
+    uint32_t tri[kTriQCap];       // leaf-order triangle index << 5 | owner lane
     float u[32], v[32];
     int ti[32];
-    uint8_t own[kTriQCap];        // owner lane
 };
 
 __device__ __forceinline__ unsigned long long hit_key(float t, int prim)
@@ -751,8 +755,7 @@ __device__ __forceinline__ void triq_push(TriQueue& q, uint32_t& tail, uint32_t 
     {
         const uint32_t bit = __ffs(tbits) - 1u;
         tbits &= tbits - 1u;
-        q.tri[pos & kTriQMask] = tbase + (leafMask ? __popc(leafMask & ((1u << bit) - 1u)) : bit);
-        q.own[pos & kTriQMask] = (uint8_t)lane;
+        q.tri[pos & kTriQMask] = ((tbase + (leafMask ? __popc(leafMask & ((1u << bit) - 1u)) : bit)) << 5) | lane;
         ++pos;
     }
     tail += __shfl_sync(FULL, x, 31);
@@ -771,8 +774,9 @@ __device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t
     int own = 0;
     if (act)
     {
-        tri = q.tri[(head + lane) & kTriQMask];
-        own = q.own[(head + lane) & kTriQMask];
+        const uint32_t e = q.tri[(head + lane) & kTriQMask];
+        tri = e >> 5;
+        own = (int)(e & 31u);
     }
     head += m;
     TravRay o;

@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
             continue;
         }
         // --- traverse until the warp has enough idle lanes ------------------
-        if (PRT_DEFER_TRIS && a.scene.leafTris == 1)
+        if (PRT_DEFER_TRIS && a.scene.deferTris)
         {
             // node visits queue their triangles; the warp tests them 32 at a
             // time, and every pending test is done before any lane shades
@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
-    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // leafTris == 1
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // deferTris
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
             if (exhausted) break;
             continue;
         }
-        if (PRT_DEFER_NEE && a.scene.leafTris == 1)
+        if (PRT_DEFER_NEE && a.scene.deferTris)
         {
             // extension rays (closest hit) and shadow rays (any hit) share the queue
             warp_trav_deferred(*tq, ts, a.scene, r, 0.0f, st, has, true, kRefillMin, lane, nullptr, nullptr, nullptr,
@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneD
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
-    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // leafTris == 1
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // deferTris
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -659,7 +659,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneD
             if (exhausted) break;
             continue;
         }
-        if (PRT_DEFER_ISECT && sc.leafTris == 1)
+        if (PRT_DEFER_ISECT && sc.deferTris)
         {
             warp_trav_deferred(*tq, ts, sc, r, tnear, st, has, !exhausted, kRefillMin, lane, nullptr, nullptr,
                                nullptr, nullptr, nullptr, kAnyHit);
@@ -773,7 +773,7 @@ __global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, f
     st.sh = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.overflow = false;
-    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // forward, leafTris == 1
+    TriQueue* tq = reinterpret_cast<TriQueue*>(s_stack + kShared * blockDim.x) + (threadIdx.x >> 5);   // forward, deferTris
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ltMask = (1u << lane) - 1u;
@@ -832,7 +832,7 @@ __global__ void __launch_bounds__(128, 8) k_replay(SceneDev sc, CameraDev cam, f
             if (exhausted) break;
             continue;
         }
-        if (PRT_DEFER_REPLAY && !kBackward && sc.leafTris == 1)
+        if (PRT_DEFER_REPLAY && !kBackward && sc.deferTris)
         {
             warp_trav_deferred(*tq, ts, sc, r, 0.0f, st, has, true, kRefillMin, lane);
         }
@@ -1065,7 +1065,7 @@ int grid_for(Kernel kernel, int block, size_t shmem, int numSMs, const LaunchCfg
 int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs, cudaStream_t s)
 {
     size_t shmem = sizeof(uint2) * kShared * cfg.block;
-    if (a.scene.leafTris == 1 && (a.Lout ? PRT_DEFER_NEE : PRT_DEFER_TRIS))
+    if (a.scene.deferTris && (a.Lout ? PRT_DEFER_NEE : PRT_DEFER_TRIS))
         shmem += sizeof(TriQueue) * (cfg.block / 32);   // the bounce kernels' triangle queues
     bool albedo = a.thrIn != nullptr || a.thrOut != nullptr;
     auto go = [&](auto kernel) {
@@ -1129,7 +1129,7 @@ int launch_intersect(const SceneDev& sc, const RayRec* rays, HitRec* hits, int n
     if (n <= 0) return 0;
     const int block = 128;
     size_t shmem = sizeof(uint2) * kShared * block;
-    if (PRT_DEFER_ISECT && sc.leafTris == 1) shmem += sizeof(TriQueue) * (block / 32);
+    if (PRT_DEFER_ISECT && sc.deferTris) shmem += sizeof(TriQueue) * (block / 32);
     LaunchCfg cfg;
     auto go = [&](auto kernel) {
         // no more warps than rays: 32 rays per warp
@@ -1204,7 +1204,7 @@ int launch_replay(const SceneDev& sc, const CameraDev& cam, float4* accum, int p
     size_t shmem = sizeof(uint2) * kShared * block;
     // the backward kernel keeps in-lane triangle tests: with its gradient table
     // in shared memory the queues would cost it occupancy (measured 17% slower)
-    if (PRT_DEFER_REPLAY && !backward && sc.leafTris == 1) shmem += sizeof(TriQueue) * (block / 32);
+    if (PRT_DEFER_REPLAY && !backward && sc.deferTris) shmem += sizeof(TriQueue) * (block / 32);
     LaunchCfg cfg;
     auto go = [&](auto kernel) {
         int grid = grid_for(kernel, block, shmem, numSMs, cfg);

@@ -1231,7 +1231,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
     std::vector<float4*> tmp((size_t)n, nullptr);
     long long total = 0;
     int maxDepth = 0;
-    int leaf1 = 1;
+    int leaf1 = 1, leafOne = 1;
     std::ostringstream key;
     key << "batch:" << n << ":" << ctx->cfg.block << ":" << ctx->cfg.blocksPerSM << ":" << ctx->cfg.pathsPerWave;
     for (int r = 0; r < n; ++r)
@@ -1253,6 +1253,7 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
         b.pathBegin = total;
         total += (long long)b.tilesX * b.tilesY * 64 * q.spp;
         if (!b.scene.deferTris) leaf1 = 0;
+        if (b.scene.leafTris != 1) leafOne = 0;
         maxDepth = std::max(maxDepth, q.maxDepth);
         key << ":" << (const void*)q.scene << "," << q.width << "x" << q.height << "," << q.spp << "," << q.maxDepth
             << "," << (const void*)q.accum;
@@ -1292,33 +1293,53 @@ int prt_render_batch(prt_ctx* ctx, const prt_request* reqs, int n, prt_render_st
         CK(cudaMemsetAsync(table[(size_t)r].accum, 0, sizeof(float4) * (size_t)reqs[r].width * reqs[r].height,
                            ctx->stream));
     long long ppw = ctx->cfg.pathsPerWave > 0 ? ctx->cfg.pathsPerWave : default_paths_per_wave(ctx);
-    int st = ensure_queues(ctx, std::min<long long>(ppw, std::max<long long>(total, 1)), false);
+    const long long waves = total > 0 ? (total + ppw - 1) / ppw : 0;
+    // waves are dealt round-robin to concurrent chains, as record_render does,
+    // so the tail of one wave's bounce launch overlaps another wave's work
+    const int chains = (int)std::max<long long>(1, std::min<long long>(chains_for(ctx), waves));
+    key << ":chains" << chains;
+    int st = ensure_queues(ctx, std::min<long long>(ppw, std::max<long long>(total, 1)), false, chains);
     if (st != PRT_OK) return st;
     auto record = [&](int& launches) -> int {
         launches = 0;
         CK(cudaMemsetAsync(ctx->dRays, 0, sizeof(unsigned long long), ctx->stream));
+        if (chains > 1)
+        {
+            CK(cudaEventRecord(ctx->forkEv, ctx->stream));
+            for (int c = 0; c < chains; ++c) CK(cudaStreamWaitEvent(ctx->side[c], ctx->forkEv, 0));
+        }
         BatchArgs a;
         a.reqs = ctx->dReqs;
         a.nreq = n;
-        a.counts = ctx->dCounts;
-        a.fetch = ctx->dFetch;
         a.rays = ctx->dRays;
         a.maxDepth = maxDepth;
         a.sky = ctx->sky;
         a.leaf1 = leaf1;
-        for (long long w0 = 0; w0 < total; w0 += ppw)
+        a.packet = leafOne && ppw % 32 == 0;
+        long long w = 0;
+        for (long long w0 = 0; w0 < total; w0 += ppw, ++w)
         {
+            const int c = (int)(w % chains);
+            cudaStream_t s = chains > 1 ? ctx->side[c] : ctx->stream;
+            a.counts = ctx->dCounts + c * kCounterStride;
+            a.fetch = ctx->dFetch + c * kCounterStride;
             a.waveBegin = w0;
             a.waveEnd = std::min(total, w0 + ppw);
-            CK(cudaMemsetAsync(ctx->dCounts, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
-            CK(cudaMemsetAsync(ctx->dFetch, 0, sizeof(int) * (kMaxDepthCap + 2), ctx->stream));
+            CK(cudaMemsetAsync(a.counts, 0, sizeof(int) * kCounterStride, s));
+            CK(cudaMemsetAsync(a.fetch, 0, sizeof(int) * kCounterStride, s));
             for (int d = 0; d <= maxDepth; ++d)
             {
-                a.qin = d == 0 ? nullptr : ctx->q[0][(d - 1) & 1];
-                a.qout = ctx->q[0][d & 1];
-                launches += launch_batch_bounce(a, d, ctx->cfg, ctx->numSMs, ctx->stream);
+                a.qin = d == 0 ? nullptr : ctx->q[c][(d - 1) & 1];
+                a.qout = ctx->q[c][d & 1];
+                launches += launch_batch_bounce(a, d, ctx->cfg, ctx->numSMs, s);
             }
         }
+        if (chains > 1)
+            for (int c = 0; c < chains; ++c)
+            {
+                CK(cudaEventRecord(ctx->joinEv[c], ctx->side[c]));
+                CK(cudaStreamWaitEvent(ctx->stream, ctx->joinEv[c], 0));
+            }
         CK(cudaGetLastError());
         return PRT_OK;
     };

@@ -250,7 +250,8 @@ struct BatchArgs
     unsigned long long* rays;
     int maxDepth;          // largest maxDepth of the batch
     float sky;
-    int leaf1;             // every request's scene has one-triangle leaves
+    int leaf1;             // every request's scene uses deferred triangle tests (one-triangle leaves)
+    int packet;            // depth 0 as warp packets: one-triangle leaves everywhere, waves start at multiples of 32
 };
 
 struct LaunchCfg

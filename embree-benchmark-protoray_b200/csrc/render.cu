@@ -308,6 +308,68 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
 #endif
 constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build accepts (32)
 
+// Warp-collective closest-hit traversal of the warp's rays as one packet (one-
+// triangle leaves; every lane of the warp calls it).  valid: this lane holds a
+// ray; vmask: the ballot of valid; stk: the warp's kPacketStack entries of
+// shared memory.  Returns this lane's closest hit (triHit -1: none).
+__device__ __forceinline__ void packet_closest_hit(const SceneDev& sc, const TravRay& r, bool valid, unsigned vmask,
+                                                   uint2* stk, unsigned lane, float& tHit, int& primHit, int& triHit)
+{
+    const unsigned FULL = 0xffffffffu;
+    const uint32_t woct = __shfl_sync(FULL, r.octinv, __ffs(vmask) - 1);
+    tHit = FLT_MAX;
+    primHit = 0x7fffffff;
+    triHit = -1;
+    if (!sc.hasRoot) return;
+    int sp = 0;
+    uint2 ng = make_uint2(0u, 0x80000000u);   // the root: one internal child at base 0
+    for (;;)
+    {
+        const uint32_t b = 31u - __clz(ng.y & 0xff000000u);
+        ng.y &= ~(1u << b);
+        const uint32_t slot = (b - 24u) ^ woct;
+        const uint32_t nodeIdx = ng.x + __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
+        if ((ng.y & 0xff000000u) && sp < kPacketStack)
+        {
+            if (lane == 0) stk[sp] = ng;
+            ++sp;
+        }
+        const uint4* qp = reinterpret_cast<const uint4*>(sc.nodes + nodeIdx);
+        uint4 q[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
+        uint32_t leafMask = 0;
+        const uint32_t hits = valid ? node_hits1(r, q, 0.0f, tHit, leafMask, woct) : 0u;
+        // this lane's leaf triangles (leaf slot j -> triBase + rank of j among the leaf slots)
+        uint32_t lb = hits & 0xffu;
+        while (lb)
+        {
+            const uint32_t bit = __ffs(lb) - 1u;
+            lb &= lb - 1u;
+            const int ti = (int)(q[1].y + __popc(leafMask & ((1u << bit) - 1u)));
+            const float4* tp = reinterpret_cast<const float4*>(sc.tris + ti);
+            const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+            const int prim = __float_as_int(v0.w);
+            float t, u, v;
+            if (tri_test(r, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), 0.0f, tHit, prim,
+                         primHit, t, u, v))
+            {
+                tHit = t;
+                primHit = prim;
+                triHit = ti;
+            }
+        }
+        ng = make_uint2(q[1].x, __reduce_or_sync(FULL, hits & 0xff000000u) | (q[0].w >> 24));
+        if (!(ng.y & 0xff000000u))
+        {
+            if (sp == 0) break;
+            __syncwarp();
+            ng = stk[--sp];
+            __syncwarp();
+        }
+    }
+}
+
 template <bool kAlbedo>
 __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_primary_packet(WaveArgs a)
 {
@@ -349,60 +411,9 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_primary_packet(W
         if (!vmask) continue;
         TravRay r;
         trav_setup(r, org, dir);
-        const uint32_t woct = __shfl_sync(FULL, r.octinv, __ffs(vmask) - 1);
-        float tHit = FLT_MAX;
-        int primHit = 0x7fffffff;
-        int triHit = -1;
-        if (a.scene.hasRoot)
-        {
-            int sp = 0;
-            uint2 ng = make_uint2(0u, 0x80000000u);   // the root: one internal child at base 0
-            for (;;)
-            {
-                const uint32_t b = 31u - __clz(ng.y & 0xff000000u);
-                ng.y &= ~(1u << b);
-                const uint32_t slot = (b - 24u) ^ woct;
-                const uint32_t nodeIdx = ng.x + __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
-                if ((ng.y & 0xff000000u) && sp < kPacketStack)
-                {
-                    if (lane == 0) stk[sp] = ng;
-                    ++sp;
-                }
-                const uint4* qp = reinterpret_cast<const uint4*>(a.scene.nodes + nodeIdx);
-                uint4 q[5];
-#pragma unroll
-                for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
-                uint32_t leafMask = 0;
-                const uint32_t hits = valid ? node_hits1(r, q, 0.0f, tHit, leafMask, woct) : 0u;
-                // this lane's leaf triangles (leaf slot j -> triBase + rank of j among the leaf slots)
-                uint32_t lb = hits & 0xffu;
-                while (lb)
-                {
-                    const uint32_t bit = __ffs(lb) - 1u;
-                    lb &= lb - 1u;
-                    const int ti = (int)(q[1].y + __popc(leafMask & ((1u << bit) - 1u)));
-                    const float4* tp = reinterpret_cast<const float4*>(a.scene.tris + ti);
-                    const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
-                    const int prim = __float_as_int(v0.w);
-                    float t, u, v;
-                    if (tri_test(r, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), 0.0f, tHit,
-                                 prim, primHit, t, u, v))
-                    {
-                        tHit = t;
-                        primHit = prim;
-                        triHit = ti;
-                    }
-                }
-                ng = make_uint2(q[1].x, __reduce_or_sync(FULL, hits & 0xff000000u) | (q[0].w >> 24));
-                if (!(ng.y & 0xff000000u))
-                {
-                    if (sp == 0) break;
-                    __syncwarp();
-                    ng = stk[--sp];
-                    __syncwarp();
-                }
-            }
-        }
+        float tHit;
+        int primHit, triHit;
+        packet_closest_hit(a.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
         // shade / append / accumulate, as k_bounce does at depth 0
         bool cont = false;
         float contrib = 0.f;
@@ -1050,6 +1061,87 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
     }
 }
 
+// Depth 0 of the batched renderer as warp packets (k_primary_packet's
+// traversal).  The 32 items a warp takes always belong to one request:
+// requests own multiples of 64 paths, and the host uses this kernel only when
+// waves start at multiples of 32 paths.
+__global__ void __launch_bounds__(128, 8) k_batch_primary_packet(BatchArgs a)
+{
+    extern __shared__ uint2 s_dyn[];
+    long long* s_begin = reinterpret_cast<long long*>(s_dyn);
+    uint2* stk = reinterpret_cast<uint2*>(s_begin + a.nreq) + (threadIdx.x >> 5) * kPacketStack;
+    for (int q = threadIdx.x; q < a.nreq; q += blockDim.x) s_begin[q] = a.reqs[q].pathBegin;
+    __syncthreads();
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const long long total = a.waveEnd - a.waveBegin;
+    unsigned long long myRays = 0;
+    for (;;)
+    {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&a.fetch[0], 32);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= total) break;
+        // the warp's request: the one whose path range holds its first item
+        const long long g0 = a.waveBegin + base;
+        int lo = 0, hi = a.nreq - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_begin[mid] <= g0) lo = mid;
+            else hi = mid - 1;
+        }
+        const int req = lo;
+        const BatchReq& R = a.reqs[req];
+        bool valid = false;
+        int pixel = 0;
+        uint32_t rng = 0;
+        float3 org = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f);
+        if (base + (long long)lane < total)
+        {
+            const long long local = g0 + lane - s_begin[req];
+            const int perPass = R.tilesX * R.tilesY * 64;
+            const int pass = (int)(local / perPass);
+            int x, y;
+            if (wave_item_pixel((int)(local - (long long)pass * perPass), R.tilesX, R.cam.width, R.cam.height, x, y))
+            {
+                valid = true;
+                pixel = x + y * R.cam.width;
+                rng = rng_seed(pass, pixel);
+                camera_ray(R.cam, x, y, rng, org, dir);
+                ++myRays;
+            }
+        }
+        const unsigned vmask = __ballot_sync(FULL, valid);
+        if (!vmask) continue;
+        TravRay r;
+        trav_setup(r, org, dir);
+        float tHit;
+        int primHit, triHit;
+        packet_closest_hit(R.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
+        bool cont = false;
+        float contrib = 0.f;
+        if (valid)
+        {
+            if (triHit < 0)
+            {
+                contrib = a.sky;   // throughput 1 at depth 0
+            }
+            else if (R.maxDepth > 0)
+            {
+                diffuse_bounce(R.scene.tris, triHit, org, dir, tHit, rng);
+                cont = true;
+            }
+        }
+        const int o = warp_append(cont, &a.counts[1]);
+        if (cont) store_path(a.qout, o, org, (req << 24) | pixel, dir, rng);
+        else if (valid) red_add_v4(R.accum + pixel, contrib, contrib, contrib, 1.0f);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) myRays += __shfl_down_sync(FULL, myRays, off);
+    if (lane == 0 && myRays) atomicAdd(a.rays, myRays);
+}
+
 template <class Kernel>
 int grid_for(Kernel kernel, int block, size_t shmem, int numSMs, const LaunchCfg& cfg)
 {
@@ -1118,6 +1210,13 @@ int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int
         int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);
         kernel<<<grid, cfg.block, shmem, s>>>(a, depth);
     };
+    if (depth == 0 && PRT_PACKET_PRIMARY && a.packet)
+    {
+        const size_t pshmem = sizeof(long long) * a.nreq + sizeof(uint2) * kPacketStack * (cfg.block / 32);
+        int grid = grid_for(k_batch_primary_packet, cfg.block, pshmem, numSMs, cfg);
+        k_batch_primary_packet<<<grid, cfg.block, pshmem, s>>>(a);
+        return 1;
+    }
     if (depth == 0) go(k_batch_bounce<true>);
     else go(k_batch_bounce<false>);
     return 1;

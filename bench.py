@@ -671,6 +671,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch configuration")
+    ap.add_argument("--launch-config", default=None,
+                    help="block,blocksPerSM,pathsPerWave,chains,primaryPackets: set this launch configuration "
+                         "instead of autotuning (for profiler captures of the configuration a bench run chose)")
     ap.add_argument("--width", type=int, default=W, help="smaller frames are for profiling captures only")
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
@@ -699,6 +702,9 @@ def main():
         c, _ = make_ctx(prt, mesh, 0)
         c.init_frame(W, H)
         c.set_view(view, W, H)
+        if args.launch_config:
+            b, per_sm, ppw, ch, pk = (int(x) for x in args.launch_config.split(","))
+            c.set_tune(b, per_sm, ppw, ch, pk)
         ms, rays = c.render_profile(SPP, DEPTH)
         print(json.dumps({"ms_per_depth": [round(float(x), 4) for x in ms], "rays_per_depth": [int(x) for x in rays]}))
         c.close()
@@ -725,11 +731,15 @@ def main():
     # queue and launch sizes from the library's autotuner, timed on this
     # workload before the warm-up
     tune = None
-    if not args.no_autotune:
+    if args.launch_config:
+        b, per_sm, ppw, ch, pk = (int(x) for x in args.launch_config.split(","))
+        ctx.set_tune(b, per_sm, ppw, ch, pk)
+    elif not args.no_autotune:
         t0 = time.perf_counter()
         tune = ctx.autotune(npass, DEPTH)
         tune = {"block": tune["blockSize"], "blocksPerSM": tune["blocksPerSM"], "pathsPerWave": tune["pathsPerWave"],
-                "chains": tune["concurrentWaves"], "tuning_s": round(time.perf_counter() - t0, 2)}
+                "chains": tune["concurrentWaves"], "primaryPackets": tune["primaryPackets"],
+                "tuning_s": round(time.perf_counter() - t0, 2)}
 
     def step(pass_base):
         ctx.set_pass(pass_base)
@@ -826,11 +836,18 @@ def main():
 
     extras = {}
     if rank == 0 and not args.no_extras:
-        extras["batched"] = run_batch(prt, torch, local)
-        extras["differentiable"] = run_fwd_bwd(prt, torch, local)
+        # each extra block carries the SM clocks sampled while it ran
+        with ClockSampler(local) as ck:
+            extras["batched"] = run_batch(prt, torch, local)
+        extras["batched"]["clocks"] = ck.summary()
+        with ClockSampler(local) as ck:
+            extras["differentiable"] = run_fwd_bwd(prt, torch, local)
+        extras["differentiable"]["clocks"] = ck.summary()
         extras["mesh_build"] = run_mesh_build(prt, torch, local)
-        extras["c2"] = run_c2(prt, torch, local, args.steps, args.warmup,
-                              0 if (args.no_cpu or world > 1) else args.cpu_seconds / 2)
+        with ClockSampler(local) as ck:
+            extras["c2"] = run_c2(prt, torch, local, args.steps, args.warmup,
+                                  0 if (args.no_cpu or world > 1) else args.cpu_seconds / 2)
+        extras["c2"]["clocks"] = ck.summary()
 
     cpu = cpu_scalar = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -1410,8 +1410,9 @@ int prt_set_tune(prt_ctx* ctx, const prt_tune* t)
 {
     if (!ctx || !t) return PRT_EINVAL;
     if (t->blockSize < 32 || t->blockSize > 128 || (t->blockSize & 31) || t->blocksPerSM < 0 || t->blocksPerSM > 64 ||
-        t->pathsPerWave < 0 || t->concurrentWaves < 0)
+        t->pathsPerWave < 0 || t->concurrentWaves < 0 || t->primaryPackets < 0 || t->primaryPackets > 1)
         return fail(ctx, PRT_EINVAL, "invalid launch configuration");
+    ctx->cfg.packet = t->primaryPackets;
     ctx->cfg.block = t->blockSize;
     ctx->cfg.blocksPerSM = t->blocksPerSM;
     ctx->cfg.pathsPerWave = t->pathsPerWave;
@@ -1427,6 +1428,7 @@ int prt_get_tune(prt_ctx* ctx, prt_tune* t)
     t->blocksPerSM = ctx->cfg.blocksPerSM;
     t->pathsPerWave = ctx->cfg.pathsPerWave;
     t->concurrentWaves = ctx->cfg.chains;
+    t->primaryPackets = ctx->cfg.packet;
     t->mray = 0;
     return PRT_OK;
 }
@@ -1482,7 +1484,7 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
         bool improved = false;
         auto consider = [&](LaunchCfg c) -> int {
             if (c.block == cur.block && c.blocksPerSM == cur.blocksPerSM && c.pathsPerWave == cur.pathsPerWave &&
-                c.chains == cur.chains)
+                c.chains == cur.chains && c.packet == cur.packet)
                 return PRT_OK;
             double m = 0;
             int s2 = measure(c, &m);
@@ -1521,6 +1523,12 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
             c.block = b;
             st = consider(c);
         }
+        for (int pk = 0; pk <= 1 && st == PRT_OK; ++pk)
+        {
+            LaunchCfg c = cur;
+            c.packet = pk;
+            st = consider(c);
+        }
         if (!improved) break;
     }
     if (st != PRT_OK)
@@ -1539,6 +1547,7 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
         best->blocksPerSM = cur.blocksPerSM;
         best->pathsPerWave = cur.pathsPerWave;
         best->concurrentWaves = cur.chains;
+        best->primaryPackets = cur.packet;
         best->mray = curM;
     }
     return PRT_OK;

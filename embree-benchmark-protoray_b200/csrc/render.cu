@@ -301,8 +301,11 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
 // tests the triangles of the leaves its own ray hits, so its result is its
 // closest hit, the same as per-lane traversal gives (exact ties go to the
 // lower primitive id either way).  Camera rays of a small pixel block visit
-// nearly the same nodes, so the lanes stay busy together where the per-lane
-// traversal of k_bounce runs 20 of 32 lanes per instruction at this depth.
+// nearly the same nodes when pixels are fine, so the lanes stay busy together
+// where the per-lane traversal of k_bounce runs 20 of 32 lanes per instruction
+// at this depth; with coarse pixels the union of the rays' nodes grows and the
+// packet loses (measured: +1.8% at 1920x1080, -26% at 480x272 on the terrain),
+// so it is a launch option (LaunchCfg::packet) the autotuner chooses.
 #ifndef PRT_PACKET_PRIMARY
 #define PRT_PACKET_PRIMARY 1
 #endif
@@ -1178,7 +1181,7 @@ int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs
         }
         return 1;
     }
-    if (depth == 0 && PRT_PACKET_PRIMARY && a.scene.leafTris == 1)
+    if (depth == 0 && PRT_PACKET_PRIMARY && cfg.packet && a.scene.leafTris == 1)
     {
         const size_t pshmem = sizeof(uint2) * kPacketStack * (cfg.block / 32);
         auto goPacket = [&](auto kernel) {
@@ -1210,7 +1213,7 @@ int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int
         int grid = grid_for(kernel, cfg.block, shmem, numSMs, cfg);
         kernel<<<grid, cfg.block, shmem, s>>>(a, depth);
     };
-    if (depth == 0 && PRT_PACKET_PRIMARY && a.packet)
+    if (depth == 0 && PRT_PACKET_PRIMARY && cfg.packet && a.packet)
     {
         const size_t pshmem = sizeof(long long) * a.nreq + sizeof(uint2) * kPacketStack * (cfg.block / 32);
         int grid = grid_for(k_batch_primary_packet, cfg.block, pshmem, numSMs, cfg);

@@ -91,7 +91,7 @@ SOUP_DTYPE = np.dtype([("v", SOUP_VERTEX_DTYPE, 3), ("matId", "<i4")])
 
 class Tune(C.Structure):
     _fields_ = [("blockSize", C.c_int), ("blocksPerSM", C.c_int), ("pathsPerWave", C.c_int),
-                ("concurrentWaves", C.c_int), ("mray", C.c_double)]
+                ("concurrentWaves", C.c_int), ("primaryPackets", C.c_int), ("mray", C.c_double)]
 
 
 _lib = None
@@ -393,16 +393,17 @@ class Context:
         t = Tune()
         self._check(self.L.prt_autotune(self.h, spp, max_depth, C.byref(t)), "prt_autotune")
         return {"blockSize": t.blockSize, "blocksPerSM": t.blocksPerSM, "pathsPerWave": t.pathsPerWave,
-                "concurrentWaves": t.concurrentWaves, "mray": t.mray}
+                "concurrentWaves": t.concurrentWaves, "primaryPackets": t.primaryPackets, "mray": t.mray}
 
     def get_tune(self) -> Dict[str, int]:
         t = Tune()
         self._check(self.L.prt_get_tune(self.h, C.byref(t)), "prt_get_tune")
         return {"blockSize": t.blockSize, "blocksPerSM": t.blocksPerSM, "pathsPerWave": t.pathsPerWave,
-                "concurrentWaves": t.concurrentWaves}
+                "concurrentWaves": t.concurrentWaves, "primaryPackets": t.primaryPackets}
 
-    def set_tune(self, block: int, per_sm: int, paths_per_wave: int, concurrent_waves: int = 0):
-        t = Tune(block, per_sm, paths_per_wave, concurrent_waves, 0.0)
+    def set_tune(self, block: int, per_sm: int, paths_per_wave: int, concurrent_waves: int = 0,
+                 primary_packets: int = 0):
+        t = Tune(block, per_sm, paths_per_wave, concurrent_waves, primary_packets, 0.0)
         self._check(self.L.prt_set_tune(self.h, C.byref(t)), "prt_set_tune")
 
     def render_noalloc(self, cam: Camera, width: int, height: int, pass0: int, spp: int, max_depth: int,

@@ -110,6 +110,8 @@ typedef struct {
     int blocksPerSM;      /* resident blocks per SM of the persistent grid */
     int pathsPerWave;     /* queue capacity (paths in flight per wave); 0 = automatic */
     int concurrentWaves;  /* waves in flight at once, 1..4 (0 keeps the current value) */
+    int primaryPackets;   /* 1: primary rays traced as warp packets (faster for fine pixels,
+                             e.g. 1080p views; slower for coarse ones); 0: per-lane (default) */
     double mray;          /* throughput measured for the winner */
 } prt_tune;
 

@@ -11,10 +11,11 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("paths_per_wave", [0, 65536])
-def test_batch_equals_individual_renders(small, paths_per_wave):
+@pytest.mark.parametrize("paths_per_wave,packets", [(0, 0), (65536, 0), (65536, 1), (0, 1)])
+def test_batch_equals_individual_renders(small, paths_per_wave, packets):
     """paths_per_wave 65536 splits the batch into several waves, which run in
-    two concurrent chains."""
+    two concurrent chains; packets 1 traces depth 0 as warp packets
+    (k_batch_primary_packet)."""
     import prt
     import scenes
     mesh0, view0 = small
@@ -33,8 +34,7 @@ def test_batch_equals_individual_renders(small, paths_per_wave):
             np.zeros((h, w, 4), np.float32)
         reqs.append({"scene": ctxs[si], "camera": prt.camera_from_view(views[si], w, h), "width": w, "height": h,
                      "spp": spp, "maxDepth": d, "accum": acc})
-    if paths_per_wave:
-        ctxs[0].set_tune(128, 0, paths_per_wave, 2)
+    ctxs[0].set_tune(128, 0, paths_per_wave, 2, packets)
     st = ctxs[0].render_batch(reqs)
     st2 = ctxs[0].render_batch(reqs)     # replayed graph gives the same result
     total = 0

@@ -167,3 +167,32 @@ def test_query_ray(ctx_small, golden):
         assert q is not None and q["primId"] == prim
         assert abs(q["dist"] - dist) <= 1e-5 * dist
         np.testing.assert_allclose(q["Ng"], ng, atol=1e-5)
+
+
+@pytest.mark.parametrize("which", ["small", "terrain"])
+def test_packet_primaries_equal_per_lane(which, small):
+    """Primary rays as warp packets (prt_tune.primaryPackets = 1) give the same
+    closest hits as per-lane traversal, so whole renders agree up to the float
+    summation order of the accumulation, with equal ray counts."""
+    import prt
+    import scenes
+    if which == "small":
+        mesh, view = small
+        W, H, spp = 256, 256, 8
+    else:
+        mesh, view = scenes.terrain_scene()
+        W, H, spp = 320, 180, 4
+    c = prt.Context(0)
+    c.load_mesh(mesh.indices, mesh.positions)
+    c.build()
+    c.init_frame(W, H)
+    c.set_view(view, W, H)
+    out = []
+    for packets in (0, 1):
+        c.set_tune(128, 0, 0, 0, packets)
+        c.set_pass(0)
+        st = c.render(spp, 5, accumulate=False)
+        out.append((st["ray"], c.read_accum().copy()))
+    assert out[0][0] == out[1][0]
+    np.testing.assert_allclose(out[1][1], out[0][1], rtol=1e-5, atol=1e-5)
+    c.close()

@@ -454,9 +454,10 @@ def run_fwd_bwd(prt, torch, device):
 
 def run_c2(prt, torch, device, steps, warmup, cpu_seconds):
     """The 10.24M-triangle icosphere field at 1920x1080, 16 spp, maxDepth 8:
-    build time of a context's first BVH build and of a rebuild, device and
-    end-to-end Mrays/s (L2 flushed between timed steps), and the reference's
-    diffuseStream on the host cores on the same scene and camera."""
+    build time of a context's first BVH build and of a rebuild, the
+    autotuner's launch configuration for it, device and end-to-end Mrays/s (L2
+    flushed between timed steps), and the reference's diffuseStream on the
+    host cores on the same scene and camera."""
     import scenes
     mesh, _ = scenes.spheres10m_scene()
     view = scenes.field_view(mesh)
@@ -467,6 +468,11 @@ def run_c2(prt, torch, device, steps, warmup, cpu_seconds):
     c.init_frame(C2_W, C2_H)
     cam = prt.camera_from_view(view, C2_W, C2_H)
     c.set_camera(cam)
+    t0 = time.perf_counter()
+    tn = c.autotune(C2_SPP, C2_DEPTH)
+    tune = {"block": tn["blockSize"], "blocksPerSM": tn["blocksPerSM"], "pathsPerWave": tn["pathsPerWave"],
+            "chains": tn["concurrentWaves"], "primaryPackets": tn["primaryPackets"],
+            "tuning_s": round(time.perf_counter() - t0, 2)}
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
     for _ in range(warmup):
         c.set_pass(0)
@@ -499,7 +505,7 @@ def run_c2(prt, torch, device, steps, warmup, cpu_seconds):
                    "d2h_bytes_per_step": C2_W * C2_H * 16},
            "buildMs_first": round(b0["buildMs"], 2), "buildMs": round(b1["buildMs"], 2),
            "buildMprim": round(mesh.tri_count / 1e3 / b1["buildMs"], 2), "bvh8_nodes": b1["nodeCount"],
-           "bvh8_levels": b1["levels"]}
+           "bvh8_levels": b1["levels"], "launch_config": tune}
     if cpu_seconds > 0:
         r = cpu_reference_run(1000, 1, sample_seconds=cpu_seconds, scene="spheres10m")
         if r is not None:

@@ -247,14 +247,15 @@ int prt_read_counters(prt_ctx* ctx, long long* out, int n, int reset);
 int prt_debug_fail_allocations(long long afterCount);
 
 /* --- launch configuration --- */
-/* Tunes the bounce kernels' launch configuration (paths per wave = queue
- * size, concurrent waves, resident blocks per SM, block size) for the current
- * scene, frame and camera by timing renders of `spp` passes at `maxDepth`:
- * coordinate descent from the current configuration, one parameter at a time,
- * a candidate replacing the incumbent only when it is more than 1% faster.
+/* Tunes the bounce kernels' launch configuration (primary rays per lane or as
+ * warp packets, paths per wave = queue size, concurrent waves, resident blocks
+ * per SM, block size) for the current scene, frame and camera by timing
+ * renders of `spp` passes at `maxDepth`: coordinate descent from the current
+ * configuration, one parameter at a time, a candidate replacing the incumbent
+ * only when it is more than 0.3% faster.
  * Keeps the winner for later renders (see prt_get_tune), then clears the frame
  * and the pass counter.  The renders it times are the caller's workload, so a
- * call costs about 20-40 renders of it. */
+ * call costs about 60 to 170 renders of it. */
 int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best);
 int prt_set_tune(prt_ctx* ctx, const prt_tune* tune);
 int prt_get_tune(prt_ctx* ctx, prt_tune* tune);

@@ -31,7 +31,9 @@ struct TopSplit
     int bin;        // left: bins 0..bin
     int nl;         // triangles going left
     int pad;
-    float cmin[2][3], cmax[2][3];   // centroid bounds of the two halves
+    // centroid bounds of the two halves, as order-preserving bits (ford):
+    // reduced with integer atomics by k_top_count
+    uint32_t cmin[2][3], cmax[2][3];
 };
 
 namespace {
@@ -382,11 +384,13 @@ __global__ void __launch_bounds__(kSahLeaves) k_sah_rebuild(int n, const int* __
 // the range in shared memory, then merged with atomics), its triangles are
 // partitioned into the two halves of the range, and the halves become the
 // next level's tasks, k_sah_rebuild's subtrees (2..kSahLeaves triangles) or
-// leaves.  One host read-back per level (the next tasks' count and ranges)
-// sizes the next level's launches.
+// leaves.  The halves' centroid bounds (the next level's bin ranges) are
+// gathered by the counting pass over the split, not per bin.  One host
+// read-back per level (the next tasks' count and ranges) sizes the next
+// level's launches.
 constexpr int kTopBins = 32;
 constexpr int kTopChunk = 4096;        // triangles per block of the binning and partition passes
-constexpr int kBinWords = 13;          // count, box lo/hi, centroid lo/hi (order-preserving float bits)
+constexpr int kBinWords = 7;           // count, box lo, box hi (order-preserving float bits)
 
 __device__ __forceinline__ uint32_t ford(float f)
 {
@@ -414,8 +418,8 @@ __global__ void k_top_init_bins(uint32_t* bins, int words)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x)
     {
         const int w = i % kBinWords;
-        // count 0; lo fields (1-3, 7-9) start at the largest value, hi fields at 0
-        bins[i] = w == 0 ? 0u : (((w >= 1 && w <= 3) || (w >= 7 && w <= 9)) ? 0xffffffffu : 0u);
+        // count 0; lo fields (1-3) start at the largest value, hi fields (4-6) at 0
+        bins[i] = w == 0 ? 0u : (w <= 3 ? 0xffffffffu : 0u);
     }
 }
 
@@ -430,7 +434,7 @@ __global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks
     for (int i = threadIdx.x; i < 3 * kTopBins * kBinWords; i += blockDim.x)
     {
         const int w = i % kBinWords;
-        sb[i] = w == 0 ? 0u : (((w >= 1 && w <= 3) || (w >= 7 && w <= 9)) ? 0xffffffffu : 0u);
+        sb[i] = w == 0 ? 0u : (w <= 3 ? 0xffffffffu : 0u);
     }
     __syncthreads();
     float sc[3];
@@ -445,7 +449,6 @@ __global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks
         const int i = i0 + threadIdx.x;
         const bool valid = i <= ch.z;
         uint32_t lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0, 0, 0};
-        uint32_t cq[3] = {0, 0, 0};
         float c[3] = {0.f, 0.f, 0.f};
         if (valid)
         {
@@ -457,7 +460,6 @@ __global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks
                 lo[k] = ford(bl);
                 hi[k] = ford(bh);
                 c[k] = 0.5f * (bl + bh);
-                cq[k] = ford(c[k]);
             }
         }
 #pragma unroll
@@ -465,15 +467,13 @@ __global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks
         {
             const int bin = valid ? top_bin(c[ax], tk.cmin[ax], sc[ax]) : -1;
             const unsigned peers = __match_any_sync(0xffffffffu, bin);
-            uint32_t r[13];
+            uint32_t r[7];
             r[0] = __popc(peers);
 #pragma unroll
             for (int k = 0; k < 3; ++k)
             {
                 r[1 + k] = __reduce_min_sync(peers, lo[k]);
                 r[4 + k] = __reduce_max_sync(peers, hi[k]);
-                r[7 + k] = __reduce_min_sync(peers, cq[k]);
-                r[10 + k] = __reduce_max_sync(peers, cq[k]);
             }
             if (valid && lane == (unsigned)(__ffs(peers) - 1))
             {
@@ -484,8 +484,6 @@ __global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks
                 {
                     atomicMin(w + 1 + k, r[1 + k]);
                     atomicMax(w + 4 + k, r[4 + k]);
-                    atomicMin(w + 7 + k, r[7 + k]);
-                    atomicMax(w + 10 + k, r[10 + k]);
                 }
             }
         }
@@ -499,7 +497,7 @@ __global__ void __launch_bounds__(256) k_top_bin(const int4* __restrict__ chunks
         {
             if (sb[i]) atomicAdd(g + i, sb[i]);
         }
-        else if ((w >= 1 && w <= 3) || (w >= 7 && w <= 9))
+        else if (w <= 3)
         {
             if (sb[i] != 0xffffffffu) atomicMin(g + i, sb[i]);
         }
@@ -517,7 +515,8 @@ __device__ __forceinline__ float shfl_ud(float v, int off, bool down)
 
 // One warp per task, lane b = bin b: the least-cost split over the bins of
 // the three axes (prefix and suffix boxes by warp scans; ties to the lower
-// axis, then the lower bin), and the centroid bounds of the two halves.
+// axis, then the lower bin).  The halves' centroid bounds start empty here
+// and are gathered by k_top_count.
 __global__ void k_top_split(const TopTask* __restrict__ tasks, int numTasks, const uint32_t* __restrict__ bins,
                             TopSplit* splits)
 {
@@ -608,19 +607,19 @@ __global__ void k_top_split(const TopTask* __restrict__ tasks, int numTasks, con
     }
     TopSplit sp;
     sp.pad = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            sp.cmin[h][k] = 0xffffffffu;
+            sp.cmax[h][k] = 0u;
+        }
     if (best == ~0ull)
     {
         sp.axis = -1;
         sp.bin = 0;
         sp.nl = (tk.hi - tk.lo + 1) / 2;
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-            {
-                sp.cmin[h][k] = tk.cmin[k];
-                sp.cmax[h][k] = tk.cmax[k];
-            }
     }
     else
     {
@@ -629,17 +628,7 @@ __global__ void k_top_split(const TopTask* __restrict__ tasks, int numTasks, con
         sp.bin = code % kTopBins;
         const uint32_t* w = g + (sp.axis * kTopBins + lane) * kBinWords;
         const int cnt = (int)w[0];
-        const bool left = lane <= sp.bin;
-        sp.nl = __reduce_add_sync(0xffffffffu, left ? cnt : 0);
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-        {
-            const uint32_t cl = cnt ? w[7 + k] : 0xffffffffu, chh = cnt ? w[10 + k] : 0u;
-            sp.cmin[0][k] = funord(__reduce_min_sync(0xffffffffu, left ? cl : 0xffffffffu));
-            sp.cmax[0][k] = funord(__reduce_max_sync(0xffffffffu, left ? chh : 0u));
-            sp.cmin[1][k] = funord(__reduce_min_sync(0xffffffffu, left ? 0xffffffffu : cl));
-            sp.cmax[1][k] = funord(__reduce_max_sync(0xffffffffu, left ? 0u : chh));
-        }
+        sp.nl = __reduce_add_sync(0xffffffffu, lane <= sp.bin ? cnt : 0);
     }
     if (lane == 0) splits[ti] = sp;
 }
@@ -681,8 +670,8 @@ __global__ void k_top_children(const TopTask* __restrict__ tasks, int numTasks, 
         c.pad = 0;
         for (int k = 0; k < 3; ++k)
         {
-            c.cmin[k] = sp.cmin[side][k];
-            c.cmax[k] = sp.cmax[side][k];
+            c.cmin[k] = funord(sp.cmin[side][k]);
+            c.cmax[k] = funord(sp.cmax[side][k]);
         }
         nextTasks[atomicAdd(numNext, 1)] = c;
     }
@@ -697,21 +686,67 @@ __device__ __forceinline__ int top_side(const TopTask& tk, const TopSplit& sp, f
     return top_bin(c, tk.cmin[sp.axis], sc) <= sp.bin ? 0 : 1;
 }
 
-// Triangles of each chunk that go left.
+// Triangles of each chunk that go left, and the centroid bounds of the two
+// halves (merged into the task's split record with integer atomics on the
+// order-preserving bits).
 __global__ void __launch_bounds__(256) k_top_count(const int4* __restrict__ chunks, const TopTask* __restrict__ tasks,
-                                                   const TopSplit* __restrict__ splits,
-                                                   const uint32_t* __restrict__ perm,
+                                                   TopSplit* splits, const uint32_t* __restrict__ perm,
                                                    const float* __restrict__ triBox, uint32_t* leftCount)
 {
     __shared__ int warpCount[8];
     const int4 ch = chunks[blockIdx.x];
     const TopTask tk = tasks[ch.x];
-    const TopSplit sp = splits[ch.x];
+    TopSplit sp;
+    sp.axis = splits[ch.x].axis;
+    sp.bin = splits[ch.x].bin;
+    sp.nl = splits[ch.x].nl;
     const float sc = sp.axis >= 0 ? top_scale(tk.cmin[sp.axis], tk.cmax[sp.axis]) : 0.f;
     int mine = 0;
-    for (int i = ch.y + threadIdx.x; i <= ch.z; i += blockDim.x) mine += top_side(tk, sp, sc, i, perm[i], triBox) == 0;
+    uint32_t cmin[2][3], cmax[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            cmin[h][k] = 0xffffffffu;
+            cmax[h][k] = 0u;
+        }
+    for (int i = ch.y + threadIdx.x; i <= ch.z; i += blockDim.x)
+    {
+        const uint32_t tri = perm[i];
+        const int side = top_side(tk, sp, sc, i, tri, triBox);
+        mine += side == 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            const uint32_t c = ford(0.5f * (triBox[6 * (size_t)tri + k] + triBox[6 * (size_t)tri + 3 + k]));
+            if (side == 0)
+            {
+                cmin[0][k] = min(cmin[0][k], c);
+                cmax[0][k] = max(cmax[0][k], c);
+            }
+            else
+            {
+                cmin[1][k] = min(cmin[1][k], c);
+                cmax[1][k] = max(cmax[1][k], c);
+            }
+        }
+    }
     mine = __reduce_add_sync(0xffffffffu, mine);
     if ((threadIdx.x & 31) == 0) warpCount[threadIdx.x >> 5] = mine;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            const uint32_t lo = __reduce_min_sync(0xffffffffu, cmin[h][k]);
+            const uint32_t hi = __reduce_max_sync(0xffffffffu, cmax[h][k]);
+            if ((threadIdx.x & 31) == 0)
+            {
+                if (lo != 0xffffffffu) atomicMin(&splits[ch.x].cmin[h][k], lo);
+                if (hi != 0u) atomicMax(&splits[ch.x].cmax[h][k], hi);
+            }
+        }
     __syncthreads();
     if (threadIdx.x == 0)
     {
@@ -865,13 +900,13 @@ cudaError_t sah_build_tree(int n, const float* triBox, const float* cbounds, uin
         k_top_init_bins<<<std::min(div_up(words, 256), 4 * numSMs), 256, 0, stream>>>(B.bins, words);
         k_top_bin<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], perm, triBox, B.bins);
         k_top_split<<<div_up(numTasks, 4), 128, 0, stream>>>(B.task[cur], numTasks, B.bins, B.splits);
+        k_top_count<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], B.splits, perm, triBox, B.leftCount);
         e = cudaMemsetAsync(B.counters, 0, sizeof(int), stream);
         if (e != cudaSuccess) break;
         k_top_children<<<div_up(numTasks, 128), 128, 0, stream>>>(B.task[cur], numTasks, B.splits, n,
                                                                    B.task[cur ^ 1], B.counters, B.small,
                                                                    B.counters + 1, B.counters + 2, child, range,
                                                                    parent);
-        k_top_count<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], B.splits, perm, triBox, B.leftCount);
         exclusive_scan_u32(B.leftCount, B.leftCount, B.scanSums, nch, stream);
         k_top_partition<<<nch, 256, 0, stream>>>(B.chunks, B.task[cur], B.splits, perm, triBox, B.leftCount, B.tmp);
         k_top_copy<<<nch, 256, 0, stream>>>(B.chunks, B.tmp, perm);

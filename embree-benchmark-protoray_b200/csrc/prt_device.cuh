@@ -436,7 +436,12 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
 // Returns internal hits at bits 24 + (slot ^ octinv) as node_hits does, leaf
 // hits as slot bits 0..7, and the node's leaf-slot mask in leafMask.
 // octinv: the octant code that orders the internal hit bits (the ray's own in
-// per-lane traversal; one shared by a warp in packet traversal).
+// per-lane traversal; one shared by a warp in packet traversal).  kPair: the
+// planes of two children per paired FP32 FMA (fma.rn.f32x2); faster where the
+// kernel has registers to spare for the paired coefficients (the first bounce),
+// slower where it spills (the later bounces).  Both give the same results:
+// each lane of a paired FMA is rounded once, as fmaf is.
+template <bool kPair = false>
 __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q, float tnear, float tfar,
                                                uint32_t& leafMask, uint32_t octinv)
 {
@@ -458,6 +463,24 @@ __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q,
         uint32_t nearX = nx ? hiX[h] : loX[h], farX = nx ? loX[h] : hiX[h];
         uint32_t nearY = ny ? hiY[h] : loY[h], farY = ny ? loY[h] : hiY[h];
         uint32_t nearZ = nz ? hiZ[h] : loZ[h], farZ = nz ? loZ[h] : hiZ[h];
+        if (kPair)
+        {
+#pragma unroll
+            for (int j = 0; j < 4; j += 2)
+            {
+                const float2 nX = ffma2(byte_unit(nearX, j), byte_unit(nearX, j + 1), aix, aox);
+                const float2 nY = ffma2(byte_unit(nearY, j), byte_unit(nearY, j + 1), aiy, aoy);
+                const float2 nZ = ffma2(byte_unit(nearZ, j), byte_unit(nearZ, j + 1), aiz, aoz);
+                const float2 fX = ffma2(byte_unit(farX, j), byte_unit(farX, j + 1), aix, aox);
+                const float2 fY = ffma2(byte_unit(farY, j), byte_unit(farY, j + 1), aiy, aoy);
+                const float2 fZ = ffma2(byte_unit(farZ, j), byte_unit(farZ, j + 1), aiz, aoz);
+                const float t0a = fmax3(nX.x, nY.x, fmaxf(nZ.x, tnear)), t1a = fmin3(fX.x, fY.x, fminf(fZ.x, tfarp));
+                const float t0b = fmax3(nX.y, nY.y, fmaxf(nZ.y, tnear)), t1b = fmin3(fX.y, fY.y, fminf(fZ.y, tfarp));
+                if (t0a <= t1a * 1.0000008f) c8 |= 1u << (4 * h + j);
+                if (t0b <= t1b * 1.0000008f) c8 |= 1u << (4 * h + j + 1);
+            }
+            continue;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
@@ -694,6 +717,7 @@ __device__ __forceinline__ unsigned long long hit_key(float t, int prim)
 
 // tbits: the hit leaf slots (PRT_LEAF1_HITS) with the node's leaf-slot mask in
 // leafMask, or triangle offset bits with leafMask = 0.
+template <bool kPair = false>
 __device__ __forceinline__ void trav_visit(TravState& s, const SceneDev& sc, const TravRay& r, float tnear, TravStack& st,
                                            uint32_t& tbase, uint32_t& tbits, uint32_t& leafMask,
                                            uint32_t* nodeVisits = nullptr)
@@ -712,7 +736,7 @@ __device__ __forceinline__ void trav_visit(TravState& s, const SceneDev& sc, con
     uint32_t hits;
     if (PRT_LEAF1_HITS)
     {
-        hits = node_hits1(r, q, tnear, s.tHit, leafMask, r.octinv);
+        hits = node_hits1<kPair>(r, q, tnear, s.tHit, leafMask, r.octinv);
     }
     else
     {
@@ -838,6 +862,7 @@ __device__ __forceinline__ void triq_flush(TriQueue& q, uint32_t& head, uint32_t
 // tests are still merged, which can only move the hit nearer).  The counter
 // pointers (node visits, triangle tests per lane; steps, running-lane steps and
 // flushes per warp) may be null.
+template <bool kPair = false>
 __device__ __forceinline__ void warp_trav_deferred(TriQueue& q, TravState& ts, const SceneDev& sc, const TravRay& r,
                                                    float tnear, TravStack& st, bool active, bool mayStop, int refillMin,
                                                    unsigned lane, uint32_t* cNodes = nullptr, uint32_t* cTris = nullptr,
@@ -855,7 +880,7 @@ __device__ __forceinline__ void warp_trav_deferred(TriQueue& q, TravState& ts, c
             *cLaneSteps += __popc(__ballot_sync(FULL, active && !ts.done));
             *cSteps += 1;
         }
-        if (active && !ts.done) trav_visit(ts, sc, r, tnear, st, tbase, tbits, lmask, cNodes);
+        if (active && !ts.done) trav_visit<kPair>(ts, sc, r, tnear, st, tbase, tbits, lmask, cNodes);
         if (__any_sync(FULL, tbits != 0)) triq_push(q, tail, tbase, tbits, lmask, lane);
         while (tail - head >= (uint32_t)PRT_DEFER_FLUSH)
         {

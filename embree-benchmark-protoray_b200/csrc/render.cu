@@ -92,6 +92,17 @@ __device__ __forceinline__ int warp_append(bool pred, int* counter)
 #endif
 constexpr int kRefillMin = PRT_REFILL_MIN;
 
+// Paired FP32 FMAs in the node test (node_hits1<true>) of the first-bounce
+// kernels, per-lane and packet: they have the registers for them (depth 0 of
+// the terrain 4% / 7% faster, of the 10M field 6% / 8%), while the later
+// bounces spill with them (2-3% slower) and keep single FMAs.
+#ifndef PRT_PAIRED_FIRST
+#define PRT_PAIRED_FIRST 1
+#endif
+#ifndef PRT_PAIRED_PACKET
+#define PRT_PAIRED_PACKET 1
+#endif
+
 // Minimum resident 128-thread blocks per SM requested from the compiler for
 // the bounce kernel (8 caps it at 64 registers per thread).
 #ifndef PRT_BOUNCE_MIN_BLOCKS
@@ -207,8 +218,8 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
         {
             // node visits queue their triangles; the warp tests them 32 at a
             // time, and every pending test is done before any lane shades
-            warp_trav_deferred(*tq, ts, a.scene, r, 0.0f, st, has, !exhausted, kRefillMin, lane,
-                               PRT_COUNTERS ? &cNodes : nullptr, PRT_COUNTERS ? &cTris : nullptr,
+            warp_trav_deferred<kFirst && PRT_PAIRED_FIRST>(*tq, ts, a.scene, r, 0.0f, st, has, !exhausted,
+                                                           kRefillMin, lane, PRT_COUNTERS ? &cNodes : nullptr, PRT_COUNTERS ? &cTris : nullptr,
                                PRT_COUNTERS ? &cSteps : nullptr, PRT_COUNTERS ? &cLaneSteps : nullptr,
                                PRT_COUNTERS ? &cTriIters : nullptr);
         }
@@ -315,6 +326,7 @@ constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build ac
 // triangle leaves; every lane of the warp calls it).  valid: this lane holds a
 // ray; vmask: the ballot of valid; stk: the warp's kPacketStack entries of
 // shared memory.  Returns this lane's closest hit (triHit -1: none).
+template <bool kPair>
 __device__ __forceinline__ void packet_closest_hit(const SceneDev& sc, const TravRay& r, bool valid, unsigned vmask,
                                                    uint2* stk, unsigned lane, float& tHit, int& primHit, int& triHit)
 {
@@ -342,7 +354,7 @@ __device__ __forceinline__ void packet_closest_hit(const SceneDev& sc, const Tra
 #pragma unroll
         for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
         uint32_t leafMask = 0;
-        const uint32_t hits = valid ? node_hits1(r, q, 0.0f, tHit, leafMask, woct) : 0u;
+        const uint32_t hits = valid ? node_hits1<kPair>(r, q, 0.0f, tHit, leafMask, woct) : 0u;
         // this lane's leaf triangles (leaf slot j -> triBase + rank of j among the leaf slots)
         uint32_t lb = hits & 0xffu;
         while (lb)
@@ -416,7 +428,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_primary_packet(W
         trav_setup(r, org, dir);
         float tHit;
         int primHit, triHit;
-        packet_closest_hit(a.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
+        packet_closest_hit<PRT_PAIRED_PACKET>(a.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
         // shade / append / accumulate, as k_bounce does at depth 0
         bool cont = false;
         float contrib = 0.f;
@@ -1121,7 +1133,7 @@ __global__ void __launch_bounds__(128, 8) k_batch_primary_packet(BatchArgs a)
         trav_setup(r, org, dir);
         float tHit;
         int primHit, triHit;
-        packet_closest_hit(R.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
+        packet_closest_hit<PRT_PAIRED_PACKET>(R.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
         bool cont = false;
         float contrib = 0.f;
         if (valid)

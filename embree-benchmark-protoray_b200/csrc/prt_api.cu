@@ -212,6 +212,26 @@ __global__ void k_check_indices(const int* __restrict__ idx, long long n3, int n
     if ((threadIdx.x & 31) == 0 && count) atomicAdd(bad, count);
 }
 
+// Frees the path queues (the next render allocates what it needs).
+void release_queues(prt_ctx* ctx)
+{
+    for (int c = 0; c < kMaxChains; ++c)
+        for (int i = 0; i < 2; ++i)
+        {
+            cudaFree(ctx->q[c][i]);
+            cudaFree(ctx->thr[c][i]);
+            cudaFree(ctx->Lq[c][i]);
+            ctx->q[c][i] = nullptr;
+            ctx->thr[c][i] = nullptr;
+            ctx->Lq[c][i] = nullptr;
+        }
+    clear_graphs(ctx);
+    ctx->queueCap = 0;
+    ctx->queueChains = 0;
+    ctx->queueThr = false;
+    ctx->queueL = false;
+}
+
 int ensure_queues(prt_ctx* ctx, long long paths, bool withThr, int chains = 1, bool withL = false)
 {
     if (paths <= ctx->queueCap && chains <= ctx->queueChains && (!withThr || ctx->queueThr) && (!withL || ctx->queueL))
@@ -1541,7 +1561,11 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
         return st;
     }
     ctx->cfg = cur;
-    clear_graphs(ctx);
+    // the candidates may have grown the queues beyond what the winner needs
+    // (up to 4 chains of 64M-path waves): free them, the next render
+    // allocates its own
+    CK(cudaStreamSynchronize(ctx->stream));
+    release_queues(ctx);
     st = prt_clear(ctx);
     if (st != PRT_OK) return st;
     if (best)

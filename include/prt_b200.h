@@ -253,9 +253,11 @@ int prt_debug_fail_allocations(long long afterCount);
  * renders of `spp` passes at `maxDepth`: coordinate descent from the current
  * configuration, one parameter at a time, a candidate replacing the incumbent
  * only when it is more than 0.3% faster.
- * Keeps the winner for later renders (see prt_get_tune), then clears the frame
- * and the pass counter.  The renders it times are the caller's workload, so a
- * call costs about 60 to 170 renders of it. */
+ * Keeps the winner for later renders (see prt_get_tune), frees the path
+ * queues the candidates grew (up to 4 chains of 64M-path waves; the next
+ * render allocates what the winner needs), then clears the frame and the pass
+ * counter.  The renders it times are the caller's workload, so a call costs
+ * about 60 to 170 renders of it. */
 int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best);
 int prt_set_tune(prt_ctx* ctx, const prt_tune* tune);
 int prt_get_tune(prt_ctx* ctx, prt_tune* tune);

@@ -463,7 +463,7 @@ __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q,
         uint32_t nearX = nx ? hiX[h] : loX[h], farX = nx ? loX[h] : hiX[h];
         uint32_t nearY = ny ? hiY[h] : loY[h], farY = ny ? loY[h] : hiY[h];
         uint32_t nearZ = nz ? hiZ[h] : loZ[h], farZ = nz ? loZ[h] : hiZ[h];
-        if (kPair)
+        if constexpr (kPair)
         {
 #pragma unroll
             for (int j = 0; j < 4; j += 2)
@@ -479,20 +479,22 @@ __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q,
                 if (t0a <= t1a * 1.0000008f) c8 |= 1u << (4 * h + j);
                 if (t0b <= t1b * 1.0000008f) c8 |= 1u << (4 * h + j + 1);
             }
-            continue;
         }
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
+        else
         {
-            float tnx = fmaf(byte_unit(nearX, j), aix, aox);
-            float tny = fmaf(byte_unit(nearY, j), aiy, aoy);
-            float tnz = fmaf(byte_unit(nearZ, j), aiz, aoz);
-            float tfx = fmaf(byte_unit(farX, j), aix, aox);
-            float tfy = fmaf(byte_unit(farY, j), aiy, aoy);
-            float tfz = fmaf(byte_unit(farZ, j), aiz, aoz);
-            float t0 = fmax3(tnx, tny, fmaxf(tnz, tnear));
-            float t1 = fmin3(tfx, tfy, fminf(tfz, tfarp));
-            if (t0 <= t1 * 1.0000008f) c8 |= 1u << (4 * h + j);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                float tnx = fmaf(byte_unit(nearX, j), aix, aox);
+                float tny = fmaf(byte_unit(nearY, j), aiy, aoy);
+                float tnz = fmaf(byte_unit(nearZ, j), aiz, aoz);
+                float tfx = fmaf(byte_unit(farX, j), aix, aox);
+                float tfy = fmaf(byte_unit(farY, j), aiy, aoy);
+                float tfz = fmaf(byte_unit(farZ, j), aiz, aoz);
+                float t0 = fmax3(tnx, tny, fmaxf(tnz, tnear));
+                float t1 = fmin3(tfx, tfy, fminf(tfz, tfarp));
+                if (t0 <= t1 * 1.0000008f) c8 |= 1u << (4 * h + j);
+            }
         }
     }
     // bit 5 of each meta byte -> one bit per slot (multiply gathers bytes 0..3 into bits 24..27)

@@ -106,6 +106,10 @@ class Oracle:
             lib.or_render_ex.restype = C.c_int64
             lib.or_render_ex.argtypes = [C.c_void_p, C.POINTER(OrCamera), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_int]
+            lib.or_render_pixels.restype = C.c_int64
+            lib.or_render_pixels.argtypes = [C.c_void_p, C.POINTER(OrCamera), C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                             C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_float, C.c_void_p,
+                                             C.c_void_p, C.c_int, C.c_int]
             lib.or_render_backward.argtypes = [C.c_void_p, C.POINTER(OrCamera), C.c_int, C.c_int, C.c_int, C.c_int,
                                                C.c_int, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_int]
@@ -194,6 +198,22 @@ class OracleScene:
                                        None if alb is None else alb.ctypes.data, C.c_float(sky), accum.ctypes.data,
                                        nthreads, int(nee))
         return accum, int(rays)
+
+    def render_pixels(self, cam: OrCamera, width: int, height: int, pixels: np.ndarray, pass0: int, npass: int,
+                      max_depth: int, albedo: Optional[np.ndarray] = None, sky: float = 1.0, nthreads: int = 0,
+                      nee: bool = False):
+        """render() at the listed pixels (x + y * width) of a width x height
+        frame only: (values (n, 4), per-pixel ray counts (n,))."""
+        px = np.ascontiguousarray(pixels, np.int32).ravel()
+        out = np.zeros((len(px), 4), np.float64)
+        rays = np.zeros(len(px), np.int64)
+        alb = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
+        r = self.o.lib.or_render_pixels(self.h, C.byref(cam), width, height, px.ctypes.data, len(px), pass0, npass,
+                                        max_depth, None if alb is None else alb.ctypes.data, C.c_float(sky),
+                                        out.ctypes.data, rays.ctypes.data, nthreads, int(nee))
+        if r < 0:
+            raise ValueError("pixel index outside the frame")
+        return out, rays
 
     def render_backward(self, cam: OrCamera, width: int, height: int, pass0: int, npass: int, max_depth: int,
                         albedo: Optional[np.ndarray], sky: float, dL_dsum: np.ndarray, nthreads: int = 0):

@@ -829,6 +829,58 @@ int64_t or_render_ex(const or_scene* s, const or_camera* cam, int W, int H, int 
     return total;
 }
 
+typedef struct {
+    const or_scene* s;
+    const or_camera* cam;
+    int W, H, pass0, npass, maxDepth, nee;
+    const float* albedo;
+    double sky;
+    const int* pixels;
+    double* out;
+    int64_t* rays;
+} pixels_ctx;
+
+/* One listed pixel, its passes in order: the same per-pixel sums as
+ * render_row (RendererSingle::renderTile, render/renderer_single.h:107-131). */
+static void render_listed_pixel(void* vctx, int i, int worker)
+{
+    (void)worker;
+    pixels_ctx* c = (pixels_ctx*)vctx;
+    int pixel = c->pixels[i];
+    int x = pixel % c->W, y = pixel / c->W;
+    int64_t rays = 0;
+    double* a = c->out + 4 * (size_t)i;
+    a[0] = a[1] = a[2] = a[3] = 0.0;
+    for (int p = 0; p < c->npass; ++p)
+    {
+        double v = c->nee ? eval_path_nee(c->s, c->cam, c->W, c->H, x, y, c->pass0 + p, c->maxDepth, c->albedo,
+                                          c->sky, &rays)
+                          : eval_path(c->s, c->cam, c->W, c->H, x, y, c->pass0 + p, c->maxDepth, c->albedo,
+                                      c->sky, &rays, NULL, NULL, NULL);
+        a[0] += v; a[1] += v; a[2] += v; a[3] += 1.0;
+    }
+    c->rays[i] = rays;
+}
+
+int64_t or_render_pixels(const or_scene* s, const or_camera* cam, int W, int H, const int* pixels, int n,
+                         int pass0, int npass, int maxDepth, const float* albedo, float sky, double* out,
+                         int64_t* rays_out, int nthreads, int nee)
+{
+    if (n <= 0) return 0;
+    for (int i = 0; i < n; ++i)
+        if (pixels[i] < 0 || (int64_t)pixels[i] >= (int64_t)W * H) return -1;
+    pixels_ctx c;
+    memset(&c, 0, sizeof(c));
+    c.s = s; c.cam = cam; c.W = W; c.H = H; c.pass0 = pass0; c.npass = npass; c.maxDepth = maxDepth;
+    c.nee = nee; c.albedo = albedo; c.sky = sky; c.pixels = pixels; c.out = out;
+    c.rays = rays_out ? rays_out : (int64_t*)calloc((size_t)n, sizeof(int64_t));
+    par_for(nthreads, n, render_listed_pixel, &c);
+    int64_t total = 0;
+    for (int i = 0; i < n; ++i) total += c.rays[i];
+    if (!rays_out) free(c.rays);
+    return total;
+}
+
 static void backward_row(void* vctx, int y, int worker)
 {
     render_ctx* c = (render_ctx*)vctx;

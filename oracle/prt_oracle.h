@@ -100,6 +100,16 @@ int64_t or_render_ex(const or_scene* s, const or_camera* cam, int width, int hei
                      int pass0, int npass, int maxDepth, const float* albedo, float sky,
                      double* accum, int nthreads, int nee);
 
+/* As or_render_ex at the n pixels listed in pixels[] (x + y * width) of a
+ * width x height frame only: out receives n * 4 doubles, the accumulation of
+ * those pixels exactly as or_render_ex would leave it, and rays_out (n
+ * entries, nullable) each pixel's closest-hit (and shadow) query count.
+ * Lets a full-resolution frame be checked at a sample of its pixels. */
+int64_t or_render_pixels(const or_scene* s, const or_camera* cam, int width, int height,
+                         const int* pixels, int n, int pass0, int npass, int maxDepth,
+                         const float* albedo, float sky, double* out, int64_t* rays_out,
+                         int nthreads, int nee);
+
 /* FP64 adjoint of or_render with respect to per-triangle albedo and sky.
  * dL_dsum: width*height*3 doubles, the gradient of the loss with respect to
  * the accumulated rgb sums.  d_albedo (triangleCount doubles) and d_sky are

@@ -132,6 +132,30 @@ def test_nee_image_matches_reference_diffuse2(golden, small, small_oracle, oracl
     assert abs(rays - golden["image_d2_rays"][0]) <= 1e-3 * rays
 
 
+@pytest.mark.parametrize("nee", [False, True])
+def test_listed_pixels_equal_full_render(small, small_oracle, oracle_mod, nee):
+    """render_pixels (the sampled-pixel checker of full-resolution frames)
+    leaves exactly the sums and ray counts that render leaves at those pixels,
+    pass range and thin lens included."""
+    import scenes
+    mesh, view = small
+    W, H, p0, spp, depth = 40, 30, 3, 3, 4
+    O = oracle_mod.Oracle()
+    tl = scenes.View(view.pos, view.angleX, view.angleY, view.fovY, 0.3, 38.0)
+    for v in (view, tl):
+        cam = O.camera(v, W, H)
+        full, rays = small_oracle.render(cam, W, H, p0, spp, depth, nee=nee)
+        px = np.array([0, W - 1, W * H - 1, W * (H - 1), 17, 5 * W + 33, 611], np.int32)
+        got, per = small_oracle.render_pixels(cam, W, H, px, p0, spp, depth, nee=nee)
+        np.testing.assert_array_equal(got, full.reshape(-1, 4)[px])
+        assert np.all(per >= spp)
+        every, per_all = small_oracle.render_pixels(cam, W, H, np.arange(W * H), p0, spp, depth, nee=nee)
+        np.testing.assert_array_equal(every, full.reshape(-1, 4))
+        assert int(per_all.sum()) == rays
+    with pytest.raises(ValueError):
+        small_oracle.render_pixels(O.camera(view, W, H), W, H, np.array([W * H]), 0, 1, 1)
+
+
 def test_oracle_adjoint_matches_finite_differences(small, small_oracle, oracle_mod):
     """The FP64 adjoint equals the derivative of the FP64 forward (paths do not
     depend on albedo, so central differences are exact up to rounding)."""

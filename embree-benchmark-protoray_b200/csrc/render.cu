@@ -92,15 +92,26 @@ __device__ __forceinline__ int warp_append(bool pred, int* counter)
 #endif
 constexpr int kRefillMin = PRT_REFILL_MIN;
 
-// Paired FP32 FMAs in the node test (node_hits1<true>) of the first-bounce
-// kernels, per-lane and packet: they have the registers for them (depth 0 of
-// the terrain 4% / 7% faster, of the 10M field 6% / 8%), while the later
-// bounces spill with them (2-3% slower) and keep single FMAs.
+// Paired FP32 FMAs in the node test (node_hits1<true>): the six plane FMAs of
+// two children become three fma.rn.f32x2.  First-bounce kernels, per-lane and
+// packet: depth 0 of the terrain 4% / 7% faster, of the 10M field 6% / 8%.
 #ifndef PRT_PAIRED_FIRST
 #define PRT_PAIRED_FIRST 1
 #endif
 #ifndef PRT_PAIRED_PACKET
 #define PRT_PAIRED_PACKET 1
+#endif
+
+// Later bounces keep only a path's origin and its traversal terms in registers
+// while the warp traverses: the pixel, RNG state and direction are read again
+// from the input queue when the lane shades.  That frees the registers the
+// paired node test needs there (with the path kept in registers it spilled and
+// ran 2-3% slower); with both, bounces 1-5 of the terrain run 3% faster.
+#ifndef PRT_RELOAD_PATH
+#define PRT_RELOAD_PATH 1
+#endif
+#ifndef PRT_PAIRED_LATER
+#define PRT_PAIRED_LATER 1
 #endif
 
 // Minimum resident 128-thread blocks per SM requested from the compiler for
@@ -155,6 +166,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
     unsigned long long cSteps = 0, cLaneSteps = 0, cTriIters = 0;       // per warp (PRT_COUNTERS)
     int pixel = 0;
     uint32_t rng = 0;
+    int qi = 0;               // input-queue index of this lane's path (PRT_RELOAD_PATH)
     float thr = 0.f;
     TravRay r;
     TravState ts;
@@ -191,6 +203,17 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
                         thr = kAlbedo ? 1.0f : a.thrConst;
                     }
                 }
+                else if (PRT_RELOAD_PATH)
+                {
+                    // L2 only: the record is read again (pixel, RNG, direction) when
+                    // the lane shades
+                    const float4* p = reinterpret_cast<const float4*>(a.qin + i);
+                    const float4 w0 = __ldcg(p), w1 = __ldcg(p + 1);
+                    org = f3(w0.x, w0.y, w0.z);
+                    dir = f3(w1.x, w1.y, w1.z);
+                    qi = i;
+                    thr = kAlbedo ? __ldcs(a.thrIn + i) : a.thrConst;
+                }
                 else
                 {
                     PathRec pr = load_path(a.qin, i);
@@ -218,10 +241,11 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
         {
             // node visits queue their triangles; the warp tests them 32 at a
             // time, and every pending test is done before any lane shades
-            warp_trav_deferred<kFirst && PRT_PAIRED_FIRST>(*tq, ts, a.scene, r, 0.0f, st, has, !exhausted,
-                                                           kRefillMin, lane, PRT_COUNTERS ? &cNodes : nullptr, PRT_COUNTERS ? &cTris : nullptr,
-                               PRT_COUNTERS ? &cSteps : nullptr, PRT_COUNTERS ? &cLaneSteps : nullptr,
-                               PRT_COUNTERS ? &cTriIters : nullptr);
+            constexpr bool kPair = kFirst ? PRT_PAIRED_FIRST : (PRT_RELOAD_PATH && PRT_PAIRED_LATER);
+            warp_trav_deferred<kPair>(*tq, ts, a.scene, r, 0.0f, st, has, !exhausted, kRefillMin, lane,
+                                      PRT_COUNTERS ? &cNodes : nullptr, PRT_COUNTERS ? &cTris : nullptr,
+                                      PRT_COUNTERS ? &cSteps : nullptr, PRT_COUNTERS ? &cLaneSteps : nullptr,
+                                      PRT_COUNTERS ? &cTriIters : nullptr);
         }
         else
         for (;;)
@@ -245,11 +269,30 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
             if (!exhausted && 32 - __popc(running) >= kRefillMin) break;
         }
         // --- finish the lanes whose traversal is complete ---------------------
+        // (the finished path's pixel, RNG state and rays are iteration-local, so
+        // only what traversal needs is carried around the loop)
         const bool fin = has && ts.done;
         bool cont = false;
         float contrib = 0.f;
+        int fpix = 0;
+        uint32_t frng = 0;
+        float3 forg = r.org, fdir = f3(0.f, 0.f, 0.f);
         if (fin)
         {
+            if (!kFirst && PRT_RELOAD_PATH)
+            {
+                const float4* p = reinterpret_cast<const float4*>(a.qin + qi);
+                const float4 w1 = __ldcs(p + 1);
+                fpix = __float_as_int(__ldcs(reinterpret_cast<const float*>(p) + 3));
+                fdir = f3(w1.x, w1.y, w1.z);
+                frng = __float_as_uint(w1.w);
+            }
+            else
+            {
+                fpix = pixel;
+                fdir = r.dir;
+                frng = rng;
+            }
             if (ts.triHit < 0)
             {
                 contrib = __fmul_rn(thr, a.sky);
@@ -257,22 +300,19 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
             else if (!final)
             {
                 if (kAlbedo) thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + ts.primHit) : 0.8f);
-                float3 org = r.org, dir = r.dir;
-                diffuse_bounce(a.scene.tris, ts.triHit, org, dir, ts.tHit, rng);
-                r.org = org;
-                r.dir = dir;
+                diffuse_bounce(a.scene.tris, ts.triHit, forg, fdir, ts.tHit, frng);
                 cont = true;
             }
         }
         int o = warp_append(cont, &a.counts[depth + 1]);
         if (cont)
         {
-            store_path(a.qout, o, r.org, pixel, r.dir, rng);
+            store_path(a.qout, o, forg, fpix, fdir, frng);
             if (kAlbedo) __stcs(a.thrOut + o, thr);
         }
         else if (fin)
         {
-            red_add_v4(a.accum + pixel, contrib, contrib, contrib, 1.0f);
+            red_add_v4(a.accum + fpix, contrib, contrib, contrib, 1.0f);
         }
         if (fin)
         {
@@ -962,6 +1002,7 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
     bool exhausted = false;
     int pixel = 0, req = 0;
     uint32_t rng = 0;
+    int qi = 0;               // input-queue index of this lane's path (PRT_RELOAD_PATH)
     TravRay r;
     TravState ts;
     ts.done = true;
@@ -1009,6 +1050,17 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
                         ++myRays;
                     }
                 }
+                else if (PRT_RELOAD_PATH)
+                {
+                    // as in k_bounce: pixel, RNG and direction are read again when
+                    // the lane shades; the request id stays (it selects the scene)
+                    const float4* p = reinterpret_cast<const float4*>(a.qin + i);
+                    const float4 w0 = __ldcg(p), w1 = __ldcg(p + 1);
+                    org = f3(w0.x, w0.y, w0.z);
+                    dir = f3(w1.x, w1.y, w1.z);
+                    req = (int)((uint32_t)__float_as_int(w0.w) >> 24);
+                    qi = i;
+                }
                 else
                 {
                     PathRec pr = load_path(a.qin, i);
@@ -1034,7 +1086,8 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
         }
         if (PRT_DEFER_TRIS && a.leaf1)
         {
-            warp_trav_deferred(*tq, ts, a.reqs[req].scene, r, 0.0f, st, has, !exhausted, kRefillMin, lane);
+            constexpr bool kPair = !kFirst && PRT_RELOAD_PATH && PRT_PAIRED_LATER;
+            warp_trav_deferred<kPair>(*tq, ts, a.reqs[req].scene, r, 0.0f, st, has, !exhausted, kRefillMin, lane);
         }
         else
         for (;;)
@@ -1047,8 +1100,25 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
         const bool fin = has && ts.done;
         bool cont = false;
         float contrib = 0.f;
+        int fpix = 0;
+        uint32_t frng = 0;
+        float3 forg = r.org, fdir = f3(0.f, 0.f, 0.f);
         if (fin)
         {
+            if (!kFirst && PRT_RELOAD_PATH)
+            {
+                const float4* p = reinterpret_cast<const float4*>(a.qin + qi);
+                const float4 w1 = __ldcs(p + 1);
+                fpix = __float_as_int(__ldcs(reinterpret_cast<const float*>(p) + 3)) & 0xffffff;
+                fdir = f3(w1.x, w1.y, w1.z);
+                frng = __float_as_uint(w1.w);
+            }
+            else
+            {
+                fpix = pixel;
+                fdir = r.dir;
+                frng = rng;
+            }
             const BatchReq& R = a.reqs[req];
             if (ts.triHit < 0)
             {
@@ -1056,16 +1126,13 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
             }
             else if (depth < R.maxDepth)
             {
-                float3 org = r.org, dir = r.dir;
-                diffuse_bounce(R.scene.tris, ts.triHit, org, dir, ts.tHit, rng);
-                r.org = org;
-                r.dir = dir;
+                diffuse_bounce(R.scene.tris, ts.triHit, forg, fdir, ts.tHit, frng);
                 cont = true;
             }
         }
         int o = warp_append(cont, &a.counts[depth + 1]);
-        if (cont) store_path(a.qout, o, r.org, (req << 24) | pixel, r.dir, rng);
-        else if (fin) red_add_v4(a.reqs[req].accum + pixel, contrib, contrib, contrib, 1.0f);
+        if (cont) store_path(a.qout, o, forg, (req << 24) | fpix, fdir, frng);
+        else if (fin) red_add_v4(a.reqs[req].accum + fpix, contrib, contrib, contrib, 1.0f);
         if (fin) has = false;
     }
     if (kFirst)

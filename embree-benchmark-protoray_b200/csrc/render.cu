@@ -114,6 +114,20 @@ constexpr int kRefillMin = PRT_REFILL_MIN;
 #define PRT_PAIRED_LATER 1
 #endif
 
+// Paired node test in the later bounces of the next-event-estimation kernel
+// (k_bounce_nee; diffuse2 on the terrain frame at 16 spp 2281 -> 2319 Mrays/s);
+// its first bounce keeps single FMAs (paired, it spills 128 bytes).
+#ifndef PRT_PAIRED_NEE
+#define PRT_PAIRED_NEE 1
+#endif
+
+// Paired node test in the any-hit ray-query kernel (k_intersect<true>): 4M
+// incoherent occlusion queries on the terrain 1.085 -> 1.024 ms; closest-hit
+// queries keep single FMAs (paired, they spill and took 1.358 instead of 1.305).
+#ifndef PRT_PAIRED_QUERY
+#define PRT_PAIRED_QUERY 1
+#endif
+
 // Minimum resident 128-thread blocks per SM requested from the compiler for
 // the bounce kernel (8 caps it at 64 registers per thread).
 #ifndef PRT_BOUNCE_MIN_BLOCKS
@@ -541,8 +555,9 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
     bool has = false, exhausted = false, shadow = false;
     int pixel = 0;
     uint32_t rng = 0;
+    int qi = 0;               // input-queue index of this lane's path (PRT_RELOAD_PATH)
+    int slot = 0;             // output-queue slot of the extension ray while its shadow ray is traced
     float thr = 0.f, L = 0.f;
-    float3 extOrg = f3(0.f, 0.f, 0.f), extDir = f3(0.f, 0.f, 1.f);
     unsigned long long shadowRays = 0;
     TravRay r;
     TravState ts;
@@ -579,6 +594,17 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
                         L = 0.0f;
                     }
                 }
+                else if (PRT_RELOAD_PATH)
+                {
+                    // pixel, RNG state and direction are read again when the lane shades
+                    const float4* p = reinterpret_cast<const float4*>(a.qin + i);
+                    const float4 w0 = __ldcg(p), w1 = __ldcg(p + 1);
+                    org = f3(w0.x, w0.y, w0.z);
+                    dir = f3(w1.x, w1.y, w1.z);
+                    qi = i;
+                    thr = kAlbedo ? __ldcs(a.thrIn + i) : a.thrConst;
+                    L = __ldcs(a.Lin + i);
+                }
                 else
                 {
                     PathRec pr = load_path(a.qin, i);
@@ -606,8 +632,9 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
         if (PRT_DEFER_NEE && a.scene.deferTris)
         {
             // extension rays (closest hit) and shadow rays (any hit) share the queue
-            warp_trav_deferred(*tq, ts, a.scene, r, 0.0f, st, has, true, kRefillMin, lane, nullptr, nullptr, nullptr,
-                               nullptr, nullptr, shadow);
+            constexpr bool kPair = !kFirst && PRT_RELOAD_PATH && PRT_PAIRED_NEE;
+            warp_trav_deferred<kPair>(*tq, ts, a.scene, r, 0.0f, st, has, true, kRefillMin, lane, nullptr, nullptr,
+                                      nullptr, nullptr, nullptr, shadow);
         }
         else
         for (;;)
@@ -617,53 +644,75 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce_nee(WaveA
             if (running == 0) break;
             if (32 - __popc(running) >= kRefillMin) break;
         }
-        bool cont = false, end = false;
-        if (has && ts.done)
+        // Extension-ray lanes that hit sample their shadow and extension rays,
+        // append the extension ray at once and keep only its queue slot while
+        // the shadow ray is traced; the radiance gathered so far is written to
+        // that slot when the shadow ray finishes.  Values of a finished path
+        // are iteration-local, so nothing else is carried around the loop.
+        const bool finExt = has && ts.done && !shadow;
+        const bool finShadow = has && ts.done && shadow;
+        bool spawn = false, end = false;
+        int fpix = 0;
+        uint32_t frng = 0;
+        float3 so = f3(0.f, 0.f, 0.f), sd = f3(0.f, 0.f, 1.f), eo = so, ed = sd;
+        if (finExt)
         {
-            if (!shadow)
+            float3 fdir;
+            if (!kFirst && PRT_RELOAD_PATH)
             {
-                if (ts.triHit < 0)
-                {
-                    L = __fadd_rn(L, __fmul_rn(__fmul_rn(thr, a.sky), missWeight));
-                    end = true;
-                }
-                else if (final)
-                {
-                    end = true;
-                }
-                else
-                {
-                    if (kAlbedo)
-                        thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + ts.primHit) : 0.8f);
-                    else
-                        thr = __fmul_rn(thr, 0.8f);
-                    HitFrame hf = hit_frame(a.scene.tris, ts.triHit, r.org, r.dir, ts.tHit);
-                    float3 so, sd;
-                    sample_bounce(hf, rng, so, sd);          // shadow ray
-                    sample_bounce(hf, rng, extOrg, extDir);  // extension ray
-                    trav_setup(r, so, sd);
-                    trav_init(ts, a.scene, FLT_MAX, st);
-                    shadow = true;
-                    ++shadowRays;
-                }
+                const float4* p = reinterpret_cast<const float4*>(a.qin + qi);
+                const float4 w1 = __ldcs(p + 1);
+                fpix = __float_as_int(__ldcs(reinterpret_cast<const float*>(p) + 3));
+                fdir = f3(w1.x, w1.y, w1.z);
+                frng = __float_as_uint(w1.w);
             }
             else
             {
-                if (ts.triHit < 0) L = __fadd_rn(L, __fmul_rn(__fmul_rn(thr, a.sky), 0.5f));
-                cont = true;
+                fpix = pixel;
+                fdir = r.dir;
+                frng = rng;
+            }
+            if (ts.triHit < 0)
+            {
+                L = __fadd_rn(L, __fmul_rn(__fmul_rn(thr, a.sky), missWeight));
+                end = true;
+            }
+            else if (final)
+            {
+                end = true;
+            }
+            else
+            {
+                if (kAlbedo)
+                    thr = __fmul_rn(thr, a.scene.albedo ? __ldg(a.scene.albedo + ts.primHit) : 0.8f);
+                else
+                    thr = __fmul_rn(thr, 0.8f);
+                HitFrame hf = hit_frame(a.scene.tris, ts.triHit, r.org, fdir, ts.tHit);
+                sample_bounce(hf, frng, so, sd);   // shadow ray
+                sample_bounce(hf, frng, eo, ed);   // extension ray
+                spawn = true;
             }
         }
-        int o = warp_append(cont, &a.counts[depth + 1]);
-        if (cont)
+        const int o = warp_append(spawn, &a.counts[depth + 1]);
+        if (spawn)
         {
-            store_path(a.qout, o, extOrg, pixel, extDir, rng);
-            __stcs(a.Lout + o, L);
+            store_path(a.qout, o, eo, fpix, ed, frng);
             if (kAlbedo) __stcs(a.thrOut + o, thr);
-            has = false;
+            slot = o;
+            trav_setup(r, so, sd);
+            trav_init(ts, a.scene, FLT_MAX, st);
+            shadow = true;
+            ++shadowRays;
         }
         else if (end)
         {
-            red_add_v4(a.accum + pixel, L, L, L, 1.0f);
+            red_add_v4(a.accum + fpix, L, L, L, 1.0f);
+            has = false;
+        }
+        if (finShadow)
+        {
+            if (ts.triHit < 0) L = __fadd_rn(L, __fmul_rn(__fmul_rn(thr, a.sky), 0.5f));
+            __stcs(a.Lout + slot, L);
             has = false;
         }
     }
@@ -727,8 +776,9 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_intersect(SceneD
         }
         if (PRT_DEFER_ISECT && sc.deferTris)
         {
-            warp_trav_deferred(*tq, ts, sc, r, tnear, st, has, !exhausted, kRefillMin, lane, nullptr, nullptr,
-                               nullptr, nullptr, nullptr, kAnyHit);
+            constexpr bool kPair = kAnyHit && PRT_PAIRED_QUERY;
+            warp_trav_deferred<kPair>(*tq, ts, sc, r, tnear, st, has, !exhausted, kRefillMin, lane, nullptr, nullptr,
+                                      nullptr, nullptr, nullptr, kAnyHit);
         }
         else
         for (;;)

@@ -438,9 +438,10 @@ __device__ __forceinline__ uint32_t node_hits(const TravRay& r, const uint4* q, 
 // octinv: the octant code that orders the internal hit bits (the ray's own in
 // per-lane traversal; one shared by a warp in packet traversal).  kPair: the
 // planes of two children per paired FP32 FMA (fma.rn.f32x2); faster where the
-// kernel has registers to spare for the paired coefficients (the first bounce),
-// slower where it spills (the later bounces).  Both give the same results:
-// each lane of a paired FMA is rounded once, as fmaf is.
+// kernel has registers to spare for the paired coefficients, slower where they
+// make it spill heavily (closest-hit ray queries, the first bounce of the
+// diffuse2 kernel).  Both give the same results: each lane of a paired FMA is
+// rounded once, as fmaf is.
 template <bool kPair = false>
 __device__ __forceinline__ uint32_t node_hits1(const TravRay& r, const uint4* q, float tnear, float tfar,
                                                uint32_t& leafMask, uint32_t octinv)

@@ -52,6 +52,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def hbm_fraction(mrays):
+    """The HBM roofline of a throughput in Mrays/s: the wavefront record
+    traffic per ray (ALGO_BYTES_PER_RAY) at that rate over the copy peak."""
+    hbm, kind = peaks()
+    achieved = mrays * 1e6 * ALGO_BYTES_PER_RAY / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "peak_kind": kind, "algorithmic_bytes_per_ray": ALGO_BYTES_PER_RAY}
+
+
 def profile_issue():
     """Warp instructions per closest-hit query of the bounce kernel on the
     headline workload, from the committed ncu summary."""
@@ -365,6 +374,7 @@ def run_batch(prt, torch, device, reps=2):
            "requests": len(work), "rays": int(best_b["ray"])}
     out["speedup"] = round(out["batched_mray"] / out["sequential_mray"], 3)
     out["speedup_vs_calls"] = round(out["batched_mray"] / out["sequential_calls_mray"], 3)
+    out["roofline"] = hbm_fraction(out["batched_mray"])
 
     # By request size class (paths = width x height x spp): each class's
     # requests as one batched launch vs one prt_render call per request, device
@@ -506,6 +516,7 @@ def run_c2(prt, torch, device, steps, warmup, cpu_seconds):
            "buildMs_first": round(b0["buildMs"], 2), "buildMs": round(b1["buildMs"], 2),
            "buildMprim": round(mesh.tri_count / 1e3 / b1["buildMs"], 2), "bvh8_nodes": b1["nodeCount"],
            "bvh8_levels": b1["levels"], "launch_config": tune}
+    out["roofline"] = hbm_fraction(out["value"])
     if cpu_seconds > 0:
         r = cpu_reference_run(1000, 1, sample_seconds=cpu_seconds, scene="spheres10m")
         if r is not None:

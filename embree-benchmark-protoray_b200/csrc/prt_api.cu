@@ -1430,7 +1430,7 @@ int prt_set_tune(prt_ctx* ctx, const prt_tune* t)
 {
     if (!ctx || !t) return PRT_EINVAL;
     if (t->blockSize < 32 || t->blockSize > 128 || (t->blockSize & 31) || t->blocksPerSM < 0 || t->blocksPerSM > 64 ||
-        t->pathsPerWave < 0 || t->concurrentWaves < 0 || t->primaryPackets < 0 || t->primaryPackets > 1)
+        t->pathsPerWave < 0 || t->concurrentWaves < 0 || t->primaryPackets < 0 || t->primaryPackets > 2)
         return fail(ctx, PRT_EINVAL, "invalid launch configuration");
     ctx->cfg.packet = t->primaryPackets;
     ctx->cfg.block = t->blockSize;
@@ -1518,7 +1518,7 @@ int prt_autotune(prt_ctx* ctx, int spp, int maxDepth, prt_tune* best)
             }
             return s2;
         };
-        for (int pk = 0; pk <= 1 && st == PRT_OK; ++pk)
+        for (int pk = 0; pk <= 2 && st == PRT_OK; ++pk)
         {
             LaunchCfg c = cur;
             c.packet = pk;

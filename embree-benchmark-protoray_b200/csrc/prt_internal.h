@@ -260,7 +260,7 @@ struct LaunchCfg
     int blocksPerSM = 0;    // 0 = as many as stay resident
     int pathsPerWave = 0;   // 0 = automatic
     int chains = 2;         // waves in flight at once (concurrent graph branches)
-    int packet = 0;         // primary rays as warp packets (one-triangle-leaf trees)
+    int packet = 0;         // primary rays as warp packets (one-triangle-leaf trees); 2: interval traversal
 };
 
 // Kernel launchers (render.cu).  Each returns the number of launches issued.

@@ -376,11 +376,172 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
 #endif
 constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build accepts (32)
 
+// Interval traversal of a packet whose rays share one direction octant.  The
+// warp tests the packet, not each ray, against a node: lane c (of 0..7) takes
+// child c and bounds the entry and exit distances of every ray of the packet
+// on each axis from the packet's origin and inverse-direction ranges (interval
+// products of [plane - omax, plane - omin] and [imin, imax]); the child is
+// entered if the largest entry bound does not pass the smallest exit bound,
+// clipped to [0, the packet's farthest closest hit].  Child planes are widened
+// by one quantization step on both sides (the per-ray test's decode error is
+// 2^-9 of a step), so a child that any ray's own test would enter is entered:
+// the packet visits a superset of the nodes its rays visit, every lane tests
+// its ray against every triangle of the entered leaves with the exact test,
+// and each lane's result is its own closest hit.  One child test per node
+// instead of one per ray and child.  A launch option (LaunchCfg::packet 2)
+// the autotuner chooses: it wins where a packet's rays stay close (fine
+// pixels, short rays; the 1080p terrain frame: 3021 against 2982 Mrays/s with
+// per-ray packet tests) and loses where they spread apart over long, often
+// missing rays (the packet culls with its farthest hit; the 10M-triangle
+// field: 2286 against 2859).  Testing each lane's own ray against a leaf's box
+// before its triangle (planes kept in shared memory) won back part of the
+// field (2580) but cost the terrain as much (2979), so it is not done.
+
+__device__ __forceinline__ float warp_min_f(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_max_f(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Bounds of (plane - o) * inv over o in [omin, omax], inv in [imin, imax].
+__device__ __forceinline__ float ia_min(float plane, float omin, float omax, float imin, float imax)
+{
+    const float d0 = plane - omax, d1 = plane - omin;
+    return fminf(fminf(d0 * imin, d0 * imax), fminf(d1 * imin, d1 * imax));
+}
+
+__device__ __forceinline__ float ia_max(float plane, float omin, float omax, float imin, float imax)
+{
+    const float d0 = plane - omax, d1 = plane - omin;
+    return fmaxf(fmaxf(d0 * imin, d0 * imax), fmaxf(d1 * imin, d1 * imax));
+}
+
+__device__ __forceinline__ void packet_closest_hit_ia(const SceneDev& sc, const TravRay& r, bool valid,
+                                                      unsigned vmask, uint32_t woct, uint2* stk, unsigned lane,
+                                                      float& tHit, int& primHit, int& triHit)
+{
+    const unsigned FULL = 0xffffffffu;
+    // packet ranges (lanes without a ray take the first ray's values)
+    const int lead = __ffs(vmask) - 1;
+    const float lox = __shfl_sync(FULL, r.org.x, lead), loy = __shfl_sync(FULL, r.org.y, lead),
+                loz = __shfl_sync(FULL, r.org.z, lead);
+    const float lix = __shfl_sync(FULL, r.inv.x, lead), liy = __shfl_sync(FULL, r.inv.y, lead),
+                liz = __shfl_sync(FULL, r.inv.z, lead);
+    const float ox = valid ? r.org.x : lox, oy = valid ? r.org.y : loy, oz = valid ? r.org.z : loz;
+    const float ix = valid ? r.inv.x : lix, iy = valid ? r.inv.y : liy, iz = valid ? r.inv.z : liz;
+    const float oxmin = warp_min_f(ox), oxmax = warp_max_f(ox);
+    const float oymin = warp_min_f(oy), oymax = warp_max_f(oy);
+    const float ozmin = warp_min_f(oz), ozmax = warp_max_f(oz);
+    const float ixmin = warp_min_f(ix), ixmax = warp_max_f(ix);
+    const float iymin = warp_min_f(iy), iymax = warp_max_f(iy);
+    const float izmin = warp_min_f(iz), izmax = warp_max_f(iz);
+    const uint32_t oct = 7u - woct;   // bit k: negative direction on axis k
+    const bool nx = (oct & 1u) != 0u, ny = (oct & 2u) != 0u, nz = (oct & 4u) != 0u;
+    const int c = (int)(lane & 7u);
+    const int cw = c >> 2, cb = c & 3;
+    float tfarP = FLT_MAX;
+    int sp = 0;
+    uint2 ng = make_uint2(0u, 0x80000000u);   // the root: one internal child at base 0
+    for (;;)
+    {
+        const uint32_t b = 31u - __clz(ng.y & 0xff000000u);
+        ng.y &= ~(1u << b);
+        const uint32_t slot = (b - 24u) ^ woct;
+        const uint32_t nodeIdx = ng.x + __popc((ng.y & 0xffu) & ((1u << slot) - 1u));
+        if ((ng.y & 0xff000000u) && sp < kPacketStack)
+        {
+            if (lane == 0) stk[sp] = ng;
+            ++sp;
+        }
+        const uint4* qp = reinterpret_cast<const uint4*>(sc.nodes + nodeIdx);
+        uint4 q[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
+        // child c of the node against the packet
+        const uint32_t e = q[0].w;
+        const float sx = __uint_as_float((e & 0xffu) << 23), sy = __uint_as_float(((e >> 8) & 0xffu) << 23),
+                    sz = __uint_as_float(((e >> 16) & 0xffu) << 23);
+        const float px = __uint_as_float(q[0].x), py = __uint_as_float(q[0].y), pz = __uint_as_float(q[0].z);
+        const float lx = fmaf(byte_f(cw ? q[2].y : q[2].x, cb) - 1.0f, sx, px);
+        const float ly = fmaf(byte_f(cw ? q[2].w : q[2].z, cb) - 1.0f, sy, py);
+        const float lz = fmaf(byte_f(cw ? q[3].y : q[3].x, cb) - 1.0f, sz, pz);
+        const float hx = fmaf(byte_f(cw ? q[3].w : q[3].z, cb) + 1.0f, sx, px);
+        const float hy = fmaf(byte_f(cw ? q[4].y : q[4].x, cb) + 1.0f, sy, py);
+        const float hz = fmaf(byte_f(cw ? q[4].w : q[4].z, cb) + 1.0f, sz, pz);
+        const float t0 = fmaxf(fmax3(ia_min(nx ? hx : lx, oxmin, oxmax, ixmin, ixmax),
+                                     ia_min(ny ? hy : ly, oymin, oymax, iymin, iymax),
+                                     ia_min(nz ? hz : lz, ozmin, ozmax, izmin, izmax)),
+                               0.0f);
+        const float t1 = fminf(fmin3(ia_max(nx ? lx : hx, oxmin, oxmax, ixmin, ixmax),
+                                     ia_max(ny ? ly : hy, oymin, oymax, iymin, iymax),
+                                     ia_max(nz ? lz : hz, ozmin, ozmax, izmin, izmax)),
+                               tfarP * 1.0000004f);
+        // relative slack of 2^-18 on both bounds: far more than the rounding of
+        // either test at any distance the planes' step margin does not cover
+        uint32_t c8 = __ballot_sync(FULL, t0 * 0.999996f <= t1 * 1.000004f) & 0xffu;
+        // non-empty slots (bit 5 of each meta byte), leaves and internal children
+        const uint32_t ne = ((((q[1].z >> 5) & 0x01010101u) * 0x01020408u) >> 24) |
+                            (((((q[1].w >> 5) & 0x01010101u) * 0x01020408u) >> 24) << 4);
+        c8 &= ne;
+        const uint32_t imask = q[0].w >> 24;
+        const uint32_t leafMask = ne & ~imask;
+        uint32_t lb = c8 & leafMask;
+        if (lb)
+        {
+            do
+            {
+                const uint32_t bit = __ffs(lb) - 1u;
+                lb &= lb - 1u;
+                const int ti = (int)(q[1].y + __popc(leafMask & ((1u << bit) - 1u)));
+                if (valid)
+                {
+                    const float4* tp = reinterpret_cast<const float4*>(sc.tris + ti);
+                    const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+                    const int prim = __float_as_int(v0.w);
+                    float t, u, v;
+                    if (tri_test(r, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), 0.0f, tHit,
+                                 prim, primHit, t, u, v))
+                    {
+                        tHit = t;
+                        primHit = prim;
+                        triHit = ti;
+                    }
+                }
+            } while (lb);
+            tfarP = __uint_as_float(__reduce_max_sync(FULL, valid ? __float_as_uint(tHit) : 0u));
+        }
+        // internal hits: bit slot -> bit slot ^ octinv, as node_hits1 orders them
+        uint32_t in8 = c8 & imask;
+        uint32_t sw = ((in8 & 0x55u) << 1) | ((in8 >> 1) & 0x55u);
+        in8 = (woct & 1u) ? sw : in8;
+        sw = ((in8 & 0x33u) << 2) | ((in8 >> 2) & 0x33u);
+        in8 = (woct & 2u) ? sw : in8;
+        sw = ((in8 & 0x0fu) << 4) | ((in8 >> 4) & 0x0fu);
+        in8 = (woct & 4u) ? sw : in8;
+        ng = make_uint2(q[1].x, (in8 << 24) | imask);
+        if (!(ng.y & 0xff000000u))
+        {
+            if (sp == 0) break;
+            __syncwarp();
+            ng = stk[--sp];
+            __syncwarp();
+        }
+    }
+}
+
 // Warp-collective closest-hit traversal of the warp's rays as one packet (one-
 // triangle leaves; every lane of the warp calls it).  valid: this lane holds a
 // ray; vmask: the ballot of valid; stk: the warp's kPacketStack entries of
 // shared memory.  Returns this lane's closest hit (triHit -1: none).
-template <bool kPair>
+template <bool kPair, bool kIA>
 __device__ __forceinline__ void packet_closest_hit(const SceneDev& sc, const TravRay& r, bool valid, unsigned vmask,
                                                    uint2* stk, unsigned lane, float& tHit, int& primHit, int& triHit)
 {
@@ -390,6 +551,11 @@ __device__ __forceinline__ void packet_closest_hit(const SceneDev& sc, const Tra
     primHit = 0x7fffffff;
     triHit = -1;
     if (!sc.hasRoot) return;
+    if (kIA && __all_sync(FULL, !valid || r.octinv == woct))
+    {
+        packet_closest_hit_ia(sc, r, valid, vmask, woct, stk, lane, tHit, primHit, triHit);
+        return;
+    }
     int sp = 0;
     uint2 ng = make_uint2(0u, 0x80000000u);   // the root: one internal child at base 0
     for (;;)
@@ -439,7 +605,7 @@ __device__ __forceinline__ void packet_closest_hit(const SceneDev& sc, const Tra
     }
 }
 
-template <bool kAlbedo>
+template <bool kAlbedo, bool kIA>
 __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_primary_packet(WaveArgs a)
 {
     extern __shared__ uint2 s_packet[];
@@ -482,7 +648,7 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_primary_packet(W
         trav_setup(r, org, dir);
         float tHit;
         int primHit, triHit;
-        packet_closest_hit<PRT_PAIRED_PACKET>(a.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
+        packet_closest_hit<PRT_PAIRED_PACKET, kIA>(a.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
         // shade / append / accumulate, as k_bounce does at depth 0
         bool cont = false;
         float contrib = 0.f;
@@ -1197,6 +1363,7 @@ __global__ void __launch_bounds__(128, 8) k_batch_bounce(BatchArgs a, int depth)
 // traversal).  The 32 items a warp takes always belong to one request:
 // requests own multiples of 64 paths, and the host uses this kernel only when
 // waves start at multiples of 32 paths.
+template <bool kIA>
 __global__ void __launch_bounds__(128, 8) k_batch_primary_packet(BatchArgs a)
 {
     extern __shared__ uint2 s_dyn[];
@@ -1250,7 +1417,7 @@ __global__ void __launch_bounds__(128, 8) k_batch_primary_packet(BatchArgs a)
         trav_setup(r, org, dir);
         float tHit;
         int primHit, triHit;
-        packet_closest_hit<PRT_PAIRED_PACKET>(R.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
+        packet_closest_hit<PRT_PAIRED_PACKET, kIA>(R.scene, r, valid, vmask, stk, lane, tHit, primHit, triHit);
         bool cont = false;
         float contrib = 0.f;
         if (valid)
@@ -1317,8 +1484,16 @@ int launch_bounce(const WaveArgs& a, int depth, const LaunchCfg& cfg, int numSMs
             int grid = grid_for(kernel, cfg.block, pshmem, numSMs, cfg);
             kernel<<<grid, cfg.block, pshmem, s>>>(a);
         };
-        if (albedo) goPacket(k_primary_packet<true>);
-        else goPacket(k_primary_packet<false>);
+        if (cfg.packet == 2)
+        {
+            if (albedo) goPacket(k_primary_packet<true, true>);
+            else goPacket(k_primary_packet<false, true>);
+        }
+        else
+        {
+            if (albedo) goPacket(k_primary_packet<true, false>);
+            else goPacket(k_primary_packet<false, false>);
+        }
         return 1;
     }
     if (depth == 0)
@@ -1345,8 +1520,12 @@ int launch_batch_bounce(const BatchArgs& a, int depth, const LaunchCfg& cfg, int
     if (depth == 0 && PRT_PACKET_PRIMARY && cfg.packet && a.packet)
     {
         const size_t pshmem = sizeof(long long) * a.nreq + sizeof(uint2) * kPacketStack * (cfg.block / 32);
-        int grid = grid_for(k_batch_primary_packet, cfg.block, pshmem, numSMs, cfg);
-        k_batch_primary_packet<<<grid, cfg.block, pshmem, s>>>(a);
+        auto goPacket = [&](auto kernel) {
+            int grid = grid_for(kernel, cfg.block, pshmem, numSMs, cfg);
+            kernel<<<grid, cfg.block, pshmem, s>>>(a);
+        };
+        if (cfg.packet == 2) goPacket(k_batch_primary_packet<true>);
+        else goPacket(k_batch_primary_packet<false>);
         return 1;
     }
     if (depth == 0) go(k_batch_bounce<true>);

@@ -111,7 +111,10 @@ typedef struct {
     int pathsPerWave;     /* queue capacity (paths in flight per wave); 0 = automatic */
     int concurrentWaves;  /* waves in flight at once, 1..4 (0 keeps the current value) */
     int primaryPackets;   /* 1: primary rays traced as warp packets (faster for fine pixels,
-                             e.g. 1080p views; slower for coarse ones); 0: per-lane (default) */
+                             e.g. 1080p views; slower for coarse ones); 2: warp packets
+                             traversed with interval bounds of the packet (one child test per
+                             node; faster still where a packet's rays stay close, slower for
+                             long, often missing rays); 0: per-lane (default) */
     double mray;          /* throughput measured for the winner */
 } prt_tune;
 

@@ -11,11 +11,11 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("paths_per_wave,packets", [(0, 0), (65536, 0), (65536, 1), (0, 1)])
+@pytest.mark.parametrize("paths_per_wave,packets", [(0, 0), (65536, 0), (65536, 1), (0, 1), (0, 2)])
 def test_batch_equals_individual_renders(small, paths_per_wave, packets):
     """paths_per_wave 65536 splits the batch into several waves, which run in
     two concurrent chains; packets 1 traces depth 0 as warp packets
-    (k_batch_primary_packet)."""
+    (k_batch_primary_packet), 2 as packets with interval node tests."""
     import prt
     import scenes
     mesh0, view0 = small

@@ -146,11 +146,12 @@ def terrain_scene(oracle_mod):
     c.close()
 
 
-# The launch configurations the autotuner picked for the two frames on a B200
+# Launch configurations the autotuner picks among for the two frames on a B200
 # (block, blocks per SM, paths per wave, concurrent wave chains, packet
 # primaries): 16-pass waves in two chains for the terrain, one-pass waves for
-# the field, packet primaries for both.
-_TUNED = {"terrain": (128, 0, 33_177_600, 2, 1), "c2": (128, 0, 0, 2, 1)}
+# the field, packet primaries with per-ray (1) or interval (2) node tests.
+_TUNED = {"terrain": [(128, 0, 33_177_600, 2, 1), (128, 0, 33_177_600, 2, 2)],
+          "c2": [(128, 0, 0, 2, 1), (128, 0, 0, 2, 2)]}
 
 
 @pytest.mark.parametrize("which", ["terrain", "c2"])
@@ -158,12 +159,13 @@ def test_full_size_frames_at_sampled_pixels(which, request, oracle_mod):
     """The benchmark's frames at their full sizes: the terrain (1920x1080,
     64 spp, maxDepth 5) and the 10.24M-triangle field (1920x1080, 16 spp,
     maxDepth 8, camera on the field's front face), each rendered whole on the
-    GPU in the default launch configuration and in the autotuned one
-    (multi-pass waves, concurrent chains, packet primaries).  The FP64 oracle
+    GPU in the default launch configuration and in the ones the autotuner
+    picks among (multi-pass waves, concurrent chains, packet primaries with
+    per-ray or interval node tests).  The FP64 oracle
     evaluates 65,536 seeded pixels plus the four corners of the same frame.
 
     * the weight channel is spp at every pixel (each path accumulated once);
-    * both configurations count the same rays and agree at every pixel up to
+    * all configurations count the same rays and agree at every pixel up to
       the float summation order of the accumulation;
     * at the sampled pixels the mean relative error against the oracle is
       below 1e-3, and a pixel differs by more than rounding (2e-5 relative;
@@ -187,16 +189,17 @@ def test_full_size_frames_at_sampled_pixels(which, request, oracle_mod):
     t0 = c.get_tune()
     default = (t0["blockSize"], t0["blocksPerSM"], t0["pathsPerWave"], t0["concurrentWaves"], t0["primaryPackets"])
     frames = []
-    for tune in (default, _TUNED[which]):
+    for tune in [default] + _TUNED[which]:
         c.set_tune(*tune)
         c.set_pass(0)
         st = c.render(spp, depth, accumulate=False)
         frames.append((st["ray"], c.read_accum().reshape(-1, 4).astype(np.float64)))
     c.set_tune(*default)
-    (rays, img), (rays_t, img_t) = frames
-    assert np.all(img[:, 3] == spp) and np.all(img_t[:, 3] == spp)
-    assert rays == rays_t
-    np.testing.assert_allclose(img_t, img, rtol=1e-5, atol=1e-5)
+    rays, img = frames[0]
+    for rays_t, img_t in frames:
+        assert np.all(img_t[:, 3] == spp)
+        assert rays_t == rays
+        np.testing.assert_allclose(img_t, img, rtol=1e-5, atol=1e-5)
 
     rng = np.random.default_rng(11)
     px = np.unique(np.concatenate([rng.choice(W * H, 65_536, replace=False),
@@ -204,7 +207,7 @@ def test_full_size_frames_at_sampled_pixels(which, request, oracle_mod):
     O = oracle_mod.Oracle()
     ref, ref_rays = s.render_pixels(O.camera(view, W, H), W, H, px, 0, spp, depth)
     assert np.all(ref[:, 3] == spp)
-    for got in (img, img_t):
+    for _, got in frames:
         g = got[px, 0]
         err = _rel_err(g, ref[:, 0])
         assert err < 1e-3, err

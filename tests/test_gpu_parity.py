@@ -171,9 +171,10 @@ def test_query_ray(ctx_small, golden):
 
 @pytest.mark.parametrize("which", ["small", "terrain"])
 def test_packet_primaries_equal_per_lane(which, small):
-    """Primary rays as warp packets (prt_tune.primaryPackets = 1) give the same
-    closest hits as per-lane traversal, so whole renders agree up to the float
-    summation order of the accumulation, with equal ray counts."""
+    """Primary rays as warp packets (prt_tune.primaryPackets = 1, and 2 with
+    interval node tests) give the same closest hits as per-lane traversal, so
+    whole renders agree up to the float summation order of the accumulation,
+    with equal ray counts."""
     import prt
     import scenes
     if which == "small":
@@ -188,11 +189,12 @@ def test_packet_primaries_equal_per_lane(which, small):
     c.init_frame(W, H)
     c.set_view(view, W, H)
     out = []
-    for packets in (0, 1):
+    for packets in (0, 1, 2):
         c.set_tune(128, 0, 0, 0, packets)
         c.set_pass(0)
         st = c.render(spp, 5, accumulate=False)
         out.append((st["ray"], c.read_accum().copy()))
-    assert out[0][0] == out[1][0]
-    np.testing.assert_allclose(out[1][1], out[0][1], rtol=1e-5, atol=1e-5)
+    for k in (1, 2):
+        assert out[k][0] == out[0][0]
+        np.testing.assert_allclose(out[k][1], out[0][1], rtol=1e-5, atol=1e-5)
     c.close()

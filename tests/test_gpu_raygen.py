@@ -11,7 +11,7 @@ RandomSampler, sampling/random_sampler.h:44-73):
   primitive ids they hit equal the oracle's at every pixel the oracle does
   not flag as grazing;
 * a maxDepth-0 render (the fused render kernel itself, per-lane or as warp
-  packets) adds 1 to a pixel whose primary ray escapes and 0 to one that hits:
+  packets, with per-ray or interval node tests) adds 1 to a pixel whose primary ray escapes and 0 to one that hits:
   its per-pixel hit/miss mask equals the oracle's at every unflagged pixel.
 
 C0 frame: 256 x 256, passes 0 and 7, pinhole and thin lens.
@@ -75,11 +75,12 @@ def test_primary_rays_match_oracle(ctx_c0, small, small_oracle, oracle_mod, lens
     assert (rp >= 0).mean() > 0.2 and (rp < 0).mean() > 0.05   # the view sees geometry and sky
 
 
-@pytest.mark.parametrize("packets", [0, 1])
+@pytest.mark.parametrize("packets", [0, 1, 2])
 @pytest.mark.parametrize("lens", [0.0, 0.3])
 @pytest.mark.parametrize("pass_", [0, 7])
 def test_depth0_render_hit_mask_matches_oracle(ctx_c0, small, small_oracle, oracle_mod, lens, pass_, packets):
-    """packets 1: depth 0 runs the warp-packet kernel (k_primary_packet)."""
+    """packets 1: depth 0 runs the warp-packet kernel (k_primary_packet); 2: its
+    interval traversal."""
     W, H = 256, 256
     view = _view(small, lens)
     ctx_c0.set_tune(128, 0, 0, 0, packets)

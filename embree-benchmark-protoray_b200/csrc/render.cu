@@ -388,10 +388,12 @@ constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build ac
 // the packet visits a superset of the nodes its rays visit, every lane tests
 // its ray against every triangle of the entered leaves with the exact test,
 // and each lane's result is its own closest hit.  One child test per node
-// instead of one per ray and child.  A launch option (LaunchCfg::packet 2)
-// the autotuner chooses: it wins where a packet's rays stay close (fine
-// pixels, short rays; the 1080p terrain frame: 3021 against 2982 Mrays/s with
-// per-ray packet tests) and loses where they spread apart over long, often
+// instead of one per ray and child; packets of a pinhole camera share one
+// origin and need half the interval products (the terrain frame 3015 -> 3060
+// Mrays/s).  A launch option (LaunchCfg::packet 2) the autotuner chooses: it
+// wins where a packet's rays stay close (fine pixels, short rays; the 1080p
+// terrain frame: 3021 against 2982 Mrays/s with per-ray packet tests, before
+// the shared-origin case) and loses where they spread apart over long, often
 // missing rays (the packet culls with its farthest hit; the 10M-triangle
 // field: 2286 against 2859).  Testing each lane's own ray against a leaf's box
 // before its triangle (planes kept in shared memory) won back part of the
@@ -411,38 +413,41 @@ __device__ __forceinline__ float warp_max_f(float v)
     return v;
 }
 
-// Bounds of (plane - o) * inv over o in [omin, omax], inv in [imin, imax].
+// Bounds of (plane - o) * inv over o in [omin, omax], inv in [imin, imax]
+// (kPoint: one origin shared by the packet, omin == omax).
+template <bool kPoint>
 __device__ __forceinline__ float ia_min(float plane, float omin, float omax, float imin, float imax)
 {
+    if (kPoint)
+    {
+        const float d = plane - omin;
+        return fminf(d * imin, d * imax);
+    }
     const float d0 = plane - omax, d1 = plane - omin;
     return fminf(fminf(d0 * imin, d0 * imax), fminf(d1 * imin, d1 * imax));
 }
 
+template <bool kPoint>
 __device__ __forceinline__ float ia_max(float plane, float omin, float omax, float imin, float imax)
 {
+    if (kPoint)
+    {
+        const float d = plane - omin;
+        return fmaxf(d * imin, d * imax);
+    }
     const float d0 = plane - omax, d1 = plane - omin;
     return fmaxf(fmaxf(d0 * imin, d0 * imax), fmaxf(d1 * imin, d1 * imax));
 }
 
-__device__ __forceinline__ void packet_closest_hit_ia(const SceneDev& sc, const TravRay& r, bool valid,
-                                                      unsigned vmask, uint32_t woct, uint2* stk, unsigned lane,
-                                                      float& tHit, int& primHit, int& triHit)
+// The traversal loop of packet_closest_hit_ia over the packet's ranges.
+template <bool kPoint>
+__device__ __forceinline__ void packet_ia_loop(const SceneDev& sc, const TravRay& r, bool valid, uint32_t woct,
+                                               uint2* stk, unsigned lane, float& tHit, int& primHit, int& triHit,
+                                               float oxmin, float oxmax, float oymin, float oymax, float ozmin,
+                                               float ozmax, float ixmin, float ixmax, float iymin, float iymax,
+                                               float izmin, float izmax)
 {
     const unsigned FULL = 0xffffffffu;
-    // packet ranges (lanes without a ray take the first ray's values)
-    const int lead = __ffs(vmask) - 1;
-    const float lox = __shfl_sync(FULL, r.org.x, lead), loy = __shfl_sync(FULL, r.org.y, lead),
-                loz = __shfl_sync(FULL, r.org.z, lead);
-    const float lix = __shfl_sync(FULL, r.inv.x, lead), liy = __shfl_sync(FULL, r.inv.y, lead),
-                liz = __shfl_sync(FULL, r.inv.z, lead);
-    const float ox = valid ? r.org.x : lox, oy = valid ? r.org.y : loy, oz = valid ? r.org.z : loz;
-    const float ix = valid ? r.inv.x : lix, iy = valid ? r.inv.y : liy, iz = valid ? r.inv.z : liz;
-    const float oxmin = warp_min_f(ox), oxmax = warp_max_f(ox);
-    const float oymin = warp_min_f(oy), oymax = warp_max_f(oy);
-    const float ozmin = warp_min_f(oz), ozmax = warp_max_f(oz);
-    const float ixmin = warp_min_f(ix), ixmax = warp_max_f(ix);
-    const float iymin = warp_min_f(iy), iymax = warp_max_f(iy);
-    const float izmin = warp_min_f(iz), izmax = warp_max_f(iz);
     const uint32_t oct = 7u - woct;   // bit k: negative direction on axis k
     const bool nx = (oct & 1u) != 0u, ny = (oct & 2u) != 0u, nz = (oct & 4u) != 0u;
     const int c = (int)(lane & 7u);
@@ -476,13 +481,13 @@ __device__ __forceinline__ void packet_closest_hit_ia(const SceneDev& sc, const 
         const float hx = fmaf(byte_f(cw ? q[3].w : q[3].z, cb) + 1.0f, sx, px);
         const float hy = fmaf(byte_f(cw ? q[4].y : q[4].x, cb) + 1.0f, sy, py);
         const float hz = fmaf(byte_f(cw ? q[4].w : q[4].z, cb) + 1.0f, sz, pz);
-        const float t0 = fmaxf(fmax3(ia_min(nx ? hx : lx, oxmin, oxmax, ixmin, ixmax),
-                                     ia_min(ny ? hy : ly, oymin, oymax, iymin, iymax),
-                                     ia_min(nz ? hz : lz, ozmin, ozmax, izmin, izmax)),
+        const float t0 = fmaxf(fmax3(ia_min<kPoint>(nx ? hx : lx, oxmin, oxmax, ixmin, ixmax),
+                                     ia_min<kPoint>(ny ? hy : ly, oymin, oymax, iymin, iymax),
+                                     ia_min<kPoint>(nz ? hz : lz, ozmin, ozmax, izmin, izmax)),
                                0.0f);
-        const float t1 = fminf(fmin3(ia_max(nx ? lx : hx, oxmin, oxmax, ixmin, ixmax),
-                                     ia_max(ny ? ly : hy, oymin, oymax, iymin, iymax),
-                                     ia_max(nz ? lz : hz, ozmin, ozmax, izmin, izmax)),
+        const float t1 = fminf(fmin3(ia_max<kPoint>(nx ? lx : hx, oxmin, oxmax, ixmin, ixmax),
+                                     ia_max<kPoint>(ny ? ly : hy, oymin, oymax, iymin, iymax),
+                                     ia_max<kPoint>(nz ? lz : hz, ozmin, ozmax, izmin, izmax)),
                                tfarP * 1.0000004f);
         // relative slack of 2^-18 on both bounds: far more than the rounding of
         // either test at any distance the planes' step margin does not cover
@@ -535,6 +540,34 @@ __device__ __forceinline__ void packet_closest_hit_ia(const SceneDev& sc, const 
             __syncwarp();
         }
     }
+}
+
+__device__ __forceinline__ void packet_closest_hit_ia(const SceneDev& sc, const TravRay& r, bool valid,
+                                                      unsigned vmask, uint32_t woct, uint2* stk, unsigned lane,
+                                                      float& tHit, int& primHit, int& triHit)
+{
+    const unsigned FULL = 0xffffffffu;
+    // packet ranges (lanes without a ray take the first ray's values)
+    const int lead = __ffs(vmask) - 1;
+    const float lox = __shfl_sync(FULL, r.org.x, lead), loy = __shfl_sync(FULL, r.org.y, lead),
+                loz = __shfl_sync(FULL, r.org.z, lead);
+    const float lix = __shfl_sync(FULL, r.inv.x, lead), liy = __shfl_sync(FULL, r.inv.y, lead),
+                liz = __shfl_sync(FULL, r.inv.z, lead);
+    const float ox = valid ? r.org.x : lox, oy = valid ? r.org.y : loy, oz = valid ? r.org.z : loz;
+    const float ix = valid ? r.inv.x : lix, iy = valid ? r.inv.y : liy, iz = valid ? r.inv.z : liz;
+    const float oxmin = warp_min_f(ox), oxmax = warp_max_f(ox);
+    const float oymin = warp_min_f(oy), oymax = warp_max_f(oy);
+    const float ozmin = warp_min_f(oz), ozmax = warp_max_f(oz);
+    const float ixmin = warp_min_f(ix), ixmax = warp_max_f(ix);
+    const float iymin = warp_min_f(iy), iymax = warp_max_f(iy);
+    const float izmin = warp_min_f(iz), izmax = warp_max_f(iz);
+    // pinhole packets share one origin: half the interval products
+    if (oxmin == oxmax && oymin == oymax && ozmin == ozmax)
+        packet_ia_loop<true>(sc, r, valid, woct, stk, lane, tHit, primHit, triHit, oxmin, oxmax, oymin, oymax, ozmin,
+                             ozmax, ixmin, ixmax, iymin, iymax, izmin, izmax);
+    else
+        packet_ia_loop<false>(sc, r, valid, woct, stk, lane, tHit, primHit, triHit, oxmin, oxmax, oymin, oymax, ozmin,
+                              ozmax, ixmin, ixmax, iymin, iymax, izmin, izmax);
 }
 
 // Warp-collective closest-hit traversal of the warp's rays as one packet (one-

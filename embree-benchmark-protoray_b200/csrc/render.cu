@@ -397,7 +397,10 @@ constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build ac
 // missing rays (the packet culls with its farthest hit; the 10M-triangle
 // field: 2286 against 2859).  Testing each lane's own ray against a leaf's box
 // before its triangle (planes kept in shared memory) won back part of the
-// field (2580) but cost the terrain as much (2979), so it is not done.
+// field (2580) but cost the terrain as much (2979), and also culling children
+// with the four side planes of a pinhole packet's frustum (built from the
+// camera basis and the packet's pixel block) cost more than it saved (terrain
+// 3063 -> 2921, field 2323 -> 2142), so neither is done.
 
 __device__ __forceinline__ float warp_min_f(float v)
 {

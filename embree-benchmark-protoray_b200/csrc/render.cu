@@ -385,9 +385,10 @@ constexpr int kPacketStack = 64;   // >= levels of the deepest tree the build ac
 
 // Interval traversal of a packet whose rays share one direction octant.  The
 // warp tests the packet, not each ray, against a node: lane c (of 0..7) takes
-// child c (with a shared origin, lanes c, c + 8 and c + 16 take its x, y and z
-// bounds, PRT_PACKET_IA_SPLIT) and bounds the entry and exit distances of every ray of the packet
-// on each axis from the packet's origin and inverse-direction ranges (interval
+// child c (with a shared origin, lanes c, c + 8 and c + 16 take its x, y and
+// z axis, PRT_PACKET_IA_SPLIT) and bounds the entry and exit distances of
+// every ray of the packet on each axis from the packet's origin and
+// inverse-direction ranges (interval
 // products of [plane - omax, plane - omin] and [imin, imax]); the child is
 // entered if the largest entry bound does not pass the smallest exit bound,
 // clipped to [0, the packet's farthest closest hit].  Child planes are widened

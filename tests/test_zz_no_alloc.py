@@ -8,8 +8,9 @@ Checked through the C ABI against prt_render, the allocating entry point, on
 two calls in a row (the second call reuses the array the first one left
 behind), within the tolerance the other image tests use for float-atomic
 reassociation: one wave, several waves (a frame that fills the array, one
-pass per wave), per-triangle albedo and the diffuse2 integrator.  This file is
-collected last on purpose."""
+pass per wave), per-triangle albedo, the diffuse2 integrator and primary rays
+as warp packets (the context's launch configuration).  This file is collected
+last on purpose."""
 
 import numpy as np
 import pytest
@@ -68,6 +69,17 @@ def test_noalloc_per_triangle_albedo(small):
     albedo = rng.uniform(0.2, 0.8, len(mesh.indices)).astype(np.float32)
     W, H = 160, 96
     ctx, cam = _context(small, W, H, albedo=albedo)
+    _check_twice(ctx, cam, W, H, spp=4, depth=5)
+    ctx.close()
+
+
+@pytest.mark.parametrize("packets", [1, 2])
+def test_noalloc_packet_primaries(small, packets):
+    """Depth 0 as warp packets with per-ray (1) or interval (2) node tests:
+    the entry point launches the context's configuration as prt_render does."""
+    W, H = 200, 120
+    ctx, cam = _context(small, W, H)
+    ctx.set_tune(128, 0, 0, 0, packets)
     _check_twice(ctx, cam, W, H, spp=4, depth=5)
     ctx.close()
 
